@@ -1,0 +1,161 @@
+/*
+ * spike_pstrsv on NVIDIA B200 (sm_100a): C ABI.
+ *
+ * Part 1 is a drop-in for the reference library's public API
+ * (cuguilke/spike_pstrsv src/spike_pstrsv.h:7-38): the same five entry points,
+ * with the same argument meaning, plus the globals its profiler links against
+ * (src/spike_pstrsv_globals.h:53-79, src/spike_pstrsv_ops.h:15 and :238).
+ * `nthreads` is the partition count P of the Spike decomposition; the same P
+ * must be passed to preprocessing and to the solve, as in the reference.
+ * Pointers may be host or device memory (classified with
+ * cudaPointerGetAttributes).  The preprocessed matrix stays resident on the
+ * GPU until the next spike_pstrsv_preproc or free_PSTRSV3 (the reference keeps
+ * it in static arrays the same way).
+ *
+ * Part 2 is a handle-based extension (spk_*) with explicit status codes, device
+ * pointers and caller streams; it has no counterpart in the reference.
+ *
+ * No MKL, CUDA or C++ types appear in any signature.
+ */
+#ifndef SPIKE_PSTRSV_B200_H
+#define SPIKE_PSTRSV_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef MKL_INT
+typedef int MKL_INT; /* 32-bit, as under the LP64 interface the reference links (Makefile.sample:15) */
+#define SPK_DEFINED_MKL_INT 1
+#endif
+
+/* ========================================================================== */
+/* Part 1: the reference API                                                   */
+/* ========================================================================== */
+
+/* Replaces spike_pstrsv_preproc (src/spike_pstrsv.h:7, src/spike_pstrsv.c:40-81).
+ * Builds the partition, dependency and spike structure of the n x n triangular
+ * CSR matrix (a, ia, ja; 0-based, columns sorted per row, diagonal first in
+ * each row for 'U' and last for 'L') on the GPU.  uplo 'L' runs the reference
+ * 'U' algorithm on the reversal mirror J L J (the reference leaves 'L' as a
+ * TODO, src/spike_pstrsv.c:234-237). */
+void spike_pstrsv_preproc(double *a, MKL_INT *ia, MKL_INT *ja, int n, int nthreads, const char uplo);
+
+/* Replaces _spike_pstrsv_preproc (src/spike_pstrsv.h:14, src/spike_pstrsv.c:83-140):
+ * as above, accumulating per-phase seconds into the *_timer_pstrsv3 globals. */
+void _spike_pstrsv_preproc(double *a, MKL_INT *ia, MKL_INT *ja, int n, int nthreads, const char uplo);
+
+/* Replaces spike_pstrsv (src/spike_pstrsv.h:21, src/spike_pstrsv.c:142-147):
+ * preprocessing followed by one solve. */
+void spike_pstrsv(const char uplo, int m, double *a, MKL_INT *ia, MKL_INT *ja, double *b, double *x,
+                  int nthreads);
+
+/* Replaces spike_pstrsv_solve (src/spike_pstrsv.h:31, src/spike_pstrsv.c:149-239):
+ * solves A x = b with the structure of the last preprocessing call.  x is
+ * written; b is left unchanged unless SPK_CLOBBER_B is set, in which case it
+ * receives the corrected right-hand side b - R_new x as the reference leaves
+ * it (src/spike_pstrsv.c:213-215). */
+void spike_pstrsv_solve(const char uplo, int m, double *b, double *x, int nthreads);
+
+/* Replaces _spike_pstrsv_solve (src/spike_pstrsv.h:38, src/spike_pstrsv.c:241-355):
+ * as above, accumulating per-phase seconds into the timer globals. */
+void _spike_pstrsv_solve(const char uplo, int m, double *b, double *x, int nthreads);
+
+/* Replaces free_PSTRSV3 (src/spike_pstrsv_ops.h:15, src/spike_pstrsv_ops.c:122-127):
+ * releases the resident preprocessed state. */
+void free_PSTRSV3(void);
+
+/* Replaces logPSTRSV3 (src/spike_pstrsv_ops.h:238, src/spike_pstrsv_ops.c:1311-1332):
+ * prints the structure summary in the reference's text format. */
+void logPSTRSV3(int nthreads);
+
+/* Flags with the reference's names and defaults (src/spike_pstrsv_ops.c:63-65). */
+extern char PSTRSV_VERBOSE;        /* 1: logPSTRSV3 after preprocessing */
+extern char FORCE_LOAD_BALANCE;    /* 1 (default): optimizeLoadBalance step */
+extern char IS_MATRIX_PARTITIONED; /* 1: use partition_starts/ends as set by the caller, then reset */
+extern char SPK_CLOBBER_B;         /* 1: write the corrected right-hand side back into b */
+
+/* Partition bounds (src/spike_pstrsv_globals.h:14-16), sized for SPK_MAX_EXPORTED_PARTS. */
+#define SPK_MAX_EXPORTED_PARTS 65536
+extern MKL_INT partition_numRows[SPK_MAX_EXPORTED_PARTS];
+extern MKL_INT partition_starts[SPK_MAX_EXPORTED_PARTS];
+extern MKL_INT partition_ends[SPK_MAX_EXPORTED_PARTS];
+extern MKL_INT numRowsReducedSystem;
+
+/* Phase timers in seconds (src/spike_pstrsv_globals.h:58-79).  The per-thread
+ * arrays keep the reference's names; the GPU phases are device-wide, so the
+ * time of a phase is stored at index 0. */
+extern double memoryAlloc_timer_pstrsv3;
+extern double preprocessD_timer_pstrsv3;
+extern double preprocessR_timer_pstrsv3;
+extern double setDependents_timer_pstrsv3;
+extern double preprocessS_timer_pstrsv3;
+extern double preprocessMappings_timer_pstrsv3;
+extern double produceCompressedR_timer_pstrsv3;
+extern double produceS_timer_pstrsv3;
+extern double produceReducedSystem_timer_pstrsv3;
+extern double init_vars_pstrsv3;
+extern double reduced_solver_timer_pstrsv3;
+extern double temp_timer[SPK_MAX_EXPORTED_PARTS];
+extern double waitBefore_timer_pstrsv3[SPK_MAX_EXPORTED_PARTS];
+extern double computeY_timer[SPK_MAX_EXPORTED_PARTS];
+extern double solveIndependent_timer[SPK_MAX_EXPORTED_PARTS];
+extern double subtract_Rx_timer[SPK_MAX_EXPORTED_PARTS];
+extern double waitAfter_timer_pstrsv3[SPK_MAX_EXPORTED_PARTS];
+extern double solveD2_timer[SPK_MAX_EXPORTED_PARTS];
+extern double solveD_timer[SPK_MAX_EXPORTED_PARTS];
+
+/* ========================================================================== */
+/* Part 2: handle API (no counterpart in the reference)                        */
+/* ========================================================================== */
+
+enum {
+    SPK_OK = 0,
+    SPK_ERR_ARG = -1,        /* invalid argument (sizes, uplo, P) */
+    SPK_ERR_INPUT = -2,      /* malformed CSR: empty row, unsorted/out-of-range column, diagonal not in place */
+    SPK_ERR_NOMEM = -3,      /* device allocation failed */
+    SPK_ERR_CUDA = -4,       /* CUDA runtime error */
+    SPK_ERR_STATE = -5,      /* no preprocessed system / mismatched m, P or uplo */
+    SPK_ERR_TOO_LARGE = -6,  /* dense spike estimate over the 16 GiB cap (reference exits, ops.c:352-360) */
+    SPK_ERR_TIMEOUT = -7     /* a bounded device wait gave up */
+};
+
+typedef struct spk_system spk_system;
+
+/* Message and code of the last failure on the calling thread. */
+const char *spk_last_error(void);
+int spk_last_error_code(void);
+
+int spk_create(spk_system **out);
+int spk_destroy(spk_system *s);
+
+/* Preprocess (a, ia, ja) into nparts partitions.  Host or device pointers.
+ * flb: FORCE_LOAD_BALANCE.  starts/ends: optional host arrays of nparts
+ * contiguous partition bounds (the IS_MATRIX_PARTITIONED path), else NULL. */
+int spk_preproc(spk_system *s, const double *a, const int *ia, const int *ja, int n, int nparts,
+                char uplo, int flb, const int *starts, const int *ends);
+
+/* Solve with device pointers b (n doubles, not modified) and x (n doubles) on
+ * `stream` (a cudaStream_t passed as void*; NULL = the legacy default stream).
+ * Asynchronous with respect to the host. */
+int spk_solve_device(spk_system *s, const double *b, double *x, void *stream);
+
+/* Solve with host or device pointers; synchronous. */
+int spk_solve(spk_system *s, const double *b, double *x);
+
+/* Structure introspection (reference global names: "ID", "T2", "mapR", "S",
+ * "start_intervals", ...): copies up to `capacity` elements to host memory
+ * `dst` and stores the full element count and type code ('d' double, 'i'
+ * int32, 'q' int64, 'c' char).  dst may be NULL to query the size. */
+int spk_debug_array(const spk_system *s, const char *name, void *dst, long long capacity,
+                    long long *count, char *type);
+long long spk_debug_scalar(const spk_system *s, const char *name);
+
+/* The system used by the Part-1 entry points (NULL before the first preproc). */
+spk_system *spk_legacy_system(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPIKE_PSTRSV_B200_H */

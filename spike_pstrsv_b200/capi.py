@@ -1,0 +1,270 @@
+"""ctypes binding of libspike_pstrsv_b200.so (include/spike_pstrsv.h).
+
+The functions mirror the reference's C API one to one (src/spike_pstrsv.h:7-38):
+same names, same argument order and meaning (``nthreads`` is the partition
+count), same global flags.  Arrays may be numpy arrays (host memory) or CUDA
+tensors/objects exposing ``data_ptr()`` (device memory); the library tells them
+apart with cudaPointerGetAttributes.
+
+There is no CPU fallback: importing the package works without a GPU, but every
+call that computes needs the compiled library and a CUDA device, and raises
+otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+_lib = None
+
+
+class SpkError(RuntimeError):
+    """A library call failed; ``code`` is the spk status code."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Load the compiled library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run spike_pstrsv_b200.build.build() "
+                               "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, c, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_char, ctypes.c_double
+        L.spike_pstrsv_preproc.argtypes = [vp, vp, vp, i, i, c]
+        L._spike_pstrsv_preproc.argtypes = [vp, vp, vp, i, i, c]
+        L.spike_pstrsv.argtypes = [c, i, vp, vp, vp, vp, vp, i]
+        L.spike_pstrsv_solve.argtypes = [c, i, vp, vp, i]
+        L._spike_pstrsv_solve.argtypes = [c, i, vp, vp, i]
+        L.logPSTRSV3.argtypes = [i]
+        L.spk_last_error.restype = ctypes.c_char_p
+        L.spk_create.argtypes = [ctypes.POINTER(vp)]
+        L.spk_destroy.argtypes = [vp]
+        L.spk_preproc.argtypes = [vp, vp, vp, vp, i, i, c, i, vp, vp]
+        L.spk_solve_device.argtypes = [vp, vp, vp, vp]
+        L.spk_solve.argtypes = [vp, vp, vp]
+        L.spk_debug_array.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_longlong,
+                                      ctypes.POINTER(ctypes.c_longlong), ctypes.c_char_p]
+        L.spk_debug_scalar.restype = ctypes.c_longlong
+        L.spk_debug_scalar.argtypes = [vp, ctypes.c_char_p]
+        L.spk_legacy_system.restype = vp
+        _lib = L
+    return _lib
+
+
+def last_error() -> tuple[int, str]:
+    L = lib()
+    return int(L.spk_last_error_code()), (L.spk_last_error() or b"").decode()
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        code, msg = last_error()
+        raise SpkError(rc, msg)
+
+
+def _arr(x, dtype, keep: list, writable: bool = False):
+    """Pointer to x: a device pointer for CUDA tensors, else a contiguous host copy/view."""
+    if hasattr(x, "data_ptr") and getattr(x, "is_cuda", False):
+        if not x.is_contiguous():
+            raise ValueError("device arrays must be contiguous")
+        return x.data_ptr()
+    if hasattr(x, "data_ptr"):  # CPU tensor
+        x = x.numpy()
+    a = np.asarray(x)
+    if a.dtype != dtype or not a.flags["C_CONTIGUOUS"]:
+        if writable:
+            raise ValueError(f"output array must be contiguous {np.dtype(dtype)}")
+        a = np.ascontiguousarray(a, dtype=dtype)
+    keep.append(a)
+    return a.ctypes.data
+
+
+def _uplo(u) -> bytes:
+    return (u.encode() if isinstance(u, str) else bytes(u))[:1]
+
+
+# ---- reference API -------------------------------------------------------------
+
+def spike_pstrsv_preproc(a, ia, ja, n: int, nthreads: int, uplo: str = "U") -> None:
+    keep: list = []
+    lib().spike_pstrsv_preproc(_arr(a, np.float64, keep), _arr(ia, np.int32, keep),
+                               _arr(ja, np.int32, keep), int(n), int(nthreads), _uplo(uplo))
+
+
+def _spike_pstrsv_preproc(a, ia, ja, n: int, nthreads: int, uplo: str = "U") -> None:
+    keep: list = []
+    lib()._spike_pstrsv_preproc(_arr(a, np.float64, keep), _arr(ia, np.int32, keep),
+                                _arr(ja, np.int32, keep), int(n), int(nthreads), _uplo(uplo))
+
+
+def spike_pstrsv(uplo: str, m: int, a, ia, ja, b, x, nthreads: int) -> None:
+    keep: list = []
+    lib().spike_pstrsv(_uplo(uplo), int(m), _arr(a, np.float64, keep), _arr(ia, np.int32, keep),
+                       _arr(ja, np.int32, keep), _arr(b, np.float64, keep, True),
+                       _arr(x, np.float64, keep, True), int(nthreads))
+
+
+def spike_pstrsv_solve(uplo: str, m: int, b, x, nthreads: int) -> None:
+    keep: list = []
+    lib().spike_pstrsv_solve(_uplo(uplo), int(m), _arr(b, np.float64, keep, True),
+                             _arr(x, np.float64, keep, True), int(nthreads))
+
+
+def _spike_pstrsv_solve(uplo: str, m: int, b, x, nthreads: int) -> None:
+    keep: list = []
+    lib()._spike_pstrsv_solve(_uplo(uplo), int(m), _arr(b, np.float64, keep, True),
+                              _arr(x, np.float64, keep, True), int(nthreads))
+
+
+def free_PSTRSV3() -> None:
+    lib().free_PSTRSV3()
+
+
+def logPSTRSV3(nthreads: int) -> None:
+    lib().logPSTRSV3(int(nthreads))
+
+
+_FLAGS = ("PSTRSV_VERBOSE", "FORCE_LOAD_BALANCE", "IS_MATRIX_PARTITIONED", "SPK_CLOBBER_B")
+TIMERS = ("memoryAlloc_timer_pstrsv3", "preprocessD_timer_pstrsv3", "preprocessR_timer_pstrsv3",
+          "setDependents_timer_pstrsv3", "preprocessS_timer_pstrsv3",
+          "preprocessMappings_timer_pstrsv3", "produceCompressedR_timer_pstrsv3",
+          "produceS_timer_pstrsv3", "produceReducedSystem_timer_pstrsv3", "init_vars_pstrsv3",
+          "reduced_solver_timer_pstrsv3")
+
+
+def set_flag(name: str, value: int) -> None:
+    if name not in _FLAGS:
+        raise KeyError(name)
+    ctypes.c_int8.in_dll(lib(), name).value = int(value)
+
+
+def get_flag(name: str) -> int:
+    return int(ctypes.c_int8.in_dll(lib(), name).value)
+
+
+def get_global(name: str, index: int | None = None):
+    """Read an exported scalar/array global (timers, partition bounds, numRowsReducedSystem)."""
+    if name in ("partition_starts", "partition_ends", "partition_numRows"):
+        base = ctypes.addressof(ctypes.c_int32.in_dll(lib(), name))
+        return ctypes.c_int32.from_address(base + 4 * (index or 0)).value
+    if name == "numRowsReducedSystem":
+        return ctypes.c_int32.in_dll(lib(), name).value
+    if index is not None:
+        base = ctypes.addressof(ctypes.c_double.in_dll(lib(), name))
+        return ctypes.c_double.from_address(base + 8 * index).value
+    return ctypes.c_double.in_dll(lib(), name).value
+
+
+def set_partitions(starts, ends) -> None:
+    """Fill partition_starts/ends and raise IS_MATRIX_PARTITIONED (the reordering path)."""
+    L = lib()
+    for name, vals in (("partition_starts", starts), ("partition_ends", ends)):
+        base = ctypes.addressof(ctypes.c_int32.in_dll(L, name))
+        for k, v in enumerate(vals):
+            ctypes.c_int32.from_address(base + 4 * k).value = int(v)
+    set_flag("IS_MATRIX_PARTITIONED", 1)
+
+
+# ---- handle API ------------------------------------------------------------------
+
+_DT = {"d": np.float64, "i": np.int32, "q": np.int64, "c": np.int8}
+
+
+def _debug_array(h, name: str) -> np.ndarray:
+    L = lib()
+    cnt = ctypes.c_longlong()
+    ty = ctypes.create_string_buffer(2)
+    _check(L.spk_debug_array(h, name.encode(), None, 0, ctypes.byref(cnt), ty))
+    out = np.zeros(cnt.value, dtype=_DT[ty.value.decode()])
+    if cnt.value:
+        _check(L.spk_debug_array(h, name.encode(), out.ctypes.data, cnt.value, ctypes.byref(cnt), ty))
+    return out
+
+
+class System:
+    """One preprocessed matrix (spk_system)."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        _check(lib().spk_create(ctypes.byref(h)))
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            lib().spk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def preproc(self, a, ia, ja, n: int, nparts: int, uplo: str = "U", flb: int = 1,
+                starts=None, ends=None) -> "System":
+        keep: list = []
+        st = _arr(starts, np.int32, keep) if starts is not None else None
+        en = _arr(ends, np.int32, keep) if ends is not None else None
+        _check(lib().spk_preproc(self.h, _arr(a, np.float64, keep), _arr(ia, np.int32, keep),
+                                 _arr(ja, np.int32, keep), int(n), int(nparts), _uplo(uplo),
+                                 int(flb), st, en))
+        self.n = int(n)
+        return self
+
+    def solve(self, b, x=None):
+        """Synchronous solve; host (numpy) or device (CUDA tensor) arrays."""
+        keep: list = []
+        if x is None:
+            x = np.zeros(self.n)
+        _check(lib().spk_solve(self.h, _arr(b, np.float64, keep), _arr(x, np.float64, keep, True)))
+        return x
+
+    def solve_device(self, b_ptr: int, x_ptr: int, stream: int = 0) -> None:
+        """Asynchronous solve on device pointers and a cudaStream_t handle."""
+        _check(lib().spk_solve_device(self.h, ctypes.c_void_p(b_ptr), ctypes.c_void_p(x_ptr),
+                                      ctypes.c_void_p(stream)))
+
+    def array(self, name: str) -> np.ndarray:
+        return _debug_array(self.h, name)
+
+    def scalar(self, name: str) -> int:
+        return int(lib().spk_debug_scalar(self.h, name.encode()))
+
+    def structure(self) -> dict:
+        from_names = [
+            "partition_starts", "partition_ends", "partition_numRows",
+            "D", "ID", "JD", "starts_D", "ends_D", "starts_R", "ends_R",
+            "hasDependences", "hasReflections", "hasToCalculateSs", "isOptimizeds",
+            "numRows_S", "numCols_S", "starts_S", "ends_S", "start_intervals", "end_intervals",
+            "T2", "IT2", "JT2", "starts_D0", "ends_D0", "starts_D1", "ends_D1", "starts_D2",
+            "ends_D2", "mapR", "starts_mapR", "ends_mapR", "S", "mapReducedX", "T", "IT", "JT"]
+        out = {k: self.array(k) for k in from_names}
+        for k in ("numRowsReducedSystem", "numNnzsReducedSystem", "reducedSystemSolverStart",
+                  "isReducedSystemNecessary"):
+            out[k] = self.scalar(k)
+        return out
+
+
+def legacy_structure() -> dict:
+    """Structure of the system held by the reference-API entry points."""
+    h = lib().spk_legacy_system()
+    if not h:
+        raise SpkError(-5, "no preprocessed system")
+    s = System.__new__(System)
+    s.h = ctypes.c_void_p(h)
+    s.n = 0
+    out = s.structure()
+    s.h = None  # not owned
+    return out

@@ -1,0 +1,141 @@
+// Internal declarations shared by the sm_100a Spike triangular-solve library.
+//
+// Layout of one preprocessed system in HBM (all 0-based, int32 indices):
+//   U      : the upper-triangular CSR the Spike algorithm runs on (the input for
+//            uplo='U', the reversal mirror J L J for uplo='L').
+//   pools  : the reference's preprocessing products, bit-identical to the
+//            reference layout (spike_pstrsv_globals.h:13-55): D/ID/JD holding D
+//            and R_new, T2/IT2/JT2 holding D0|D1|D2, mapR, dense spikes S,
+//            reduced system T/IT/JT and mapReducedX.
+//   solve  : per-partition task tables, reduced-level offsets and scratch
+//            vectors used by the solve kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/spike_pstrsv.h"
+
+namespace spk {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+void set_error(int code, const char *fmt, ...);
+int last_error_code();
+
+#define SPK_CUDA(call)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            ::spk::set_error(SPK_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,   \
+                             cudaGetErrorString(e_));                                   \
+            return SPK_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+
+#define SPK_TRY(call)                     \
+    do {                                  \
+        int rc_ = (call);                 \
+        if (rc_ != SPK_OK) return rc_;    \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            set_error(SPK_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
+                      cudaGetErrorString(e));
+            return SPK_ERR_NOMEM;
+        }
+        n = count;
+        return SPK_OK;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------------------
+// one preprocessed system
+// ---------------------------------------------------------------------------
+struct Part {  // per-partition host metadata (reference names in comments)
+    int ps, pe, num;            // partition_starts / partition_ends / partition_numRows
+    int si, ei;                 // start_intervals / end_intervals
+    int minDR, maxIR;           // first dependent row / last coupling row (global)
+    char hasDep, hasRefl, hasS, isOpt;
+    int nRowsS, nColsS;         // numRows_S / numCols_S
+    long long startsS, endsS;   // starts_S / ends_S
+    int sD0, eD0, sD1, eD1, sD2, eD2;
+    int startsD, endsD, startsR, endsR;
+    int sMapR, eMapR;
+};
+
+struct SolveTask {  // one triangular sweep over rows [lo, hi) of U
+    int lo, hi;
+};
+
+}  // namespace spk
+
+struct spk_system {
+    int n = 0, nnz = 0, P = 0;
+    char uplo = 'U';
+    int flb = 1;
+    int built = 0;
+    int redNec = 0;
+    int nRed = 0, rss = 0, nnzRed = 0;
+    long long totalArea = 0;
+    int nIT2rows = 0;
+    long long nT = 0, nDpool = 0, nT2 = 0;
+    int nMapR = 0;
+    std::vector<spk::Part> parts;
+
+    // working upper-triangular CSR
+    spk::DBuf<double> ua;
+    spk::DBuf<int> uia, uja;
+    // reference-layout pools
+    spk::DBuf<double> D, T2, S, T;
+    spk::DBuf<int> ID, JD, IT2, JT2, mapR, dep, mapRedX, IT, JT;
+    // solve support
+    spk::DBuf<int> d_ps, d_pe, d_lvl;  // partition bounds; reduced row offset per partition
+    spk::DBuf<spk::SolveTask> d_tasks1, d_tasks2, d_copy2;
+    int ntasks1 = 0, ntasks2 = 0, ncopy2 = 0;
+    spk::DBuf<double> xbuf, red, rhs_u, xout_u;
+    std::vector<int> lvl_nonempty;  // partitions (descending) whose reduced rows hold entries
+    spk::DBuf<int> d_lvl_list;
+    int nlvl = 0;
+    cudaStream_t stream = nullptr;
+    int own_stream = 0;
+};
+
+namespace spk {
+
+int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int n, int P,
+               char uplo, int flb, const int *starts, const int *ends, int ptr_on_device,
+               double *phase_seconds);
+int solve(spk_system *s, const double *b, double *x, cudaStream_t stream, double *phase_seconds);
+int solve_prepare(spk_system *s);
+
+// pointer classification
+int is_device_pointer(const void *p);
+
+}  // namespace spk

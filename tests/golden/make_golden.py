@@ -1,0 +1,106 @@
+"""Generate the golden fixtures in this folder from the reference itself.
+
+Runs the reference's own sources (oracle/_ref/libspike_ref.so, built by
+``make -C oracle ref`` from the reference tree) through its C API and records,
+per case: the input CSR, the partition count, FORCE_LOAD_BALANCE, a right-hand
+side, the reference's x, and its preprocessing state (every array of the
+reference's globals that the structure tests compare).
+
+* ``small_*.npz``  full arrays (small matrices).
+* ``digest.json``  SHA-256 of every structure array plus the scalar fields, for
+  the BASELINE-sized cases (Poisson 128x128 at 4 partitions, banded 65,536 rows).
+
+'L' cases run the reference's 'U' path on the reversal mirror J L J (the
+reference's own 'L' path is unimplemented, src/spike_pstrsv.c:234-237).
+
+Usage: python tests/golden/make_golden.py   (needs the reference tree)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+import oracle  # noqa: E402
+from cases import rand_upper  # noqa: E402
+from spike_pstrsv_b200 import synth  # noqa: E402
+
+
+def run_reference(A, P, uplo, flb, b):
+    R = oracle.Reference()
+    U = A if uplo == "U" else synth.mirror(A)
+    R.preproc(U, P, flb=flb)
+    st = R.structure()
+    bu = b if uplo == "U" else b[::-1].copy()
+    x = R.solve(bu)
+    if uplo == "L":
+        x = x[::-1].copy()
+    return st, x
+
+
+def digest(arr: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(arr).tobytes()).hexdigest()
+
+
+def small_cases():
+    out = []
+    L = synth.poisson2d_lower(32)
+    out.append(("small_poisson32_L_P4", L, 4, "L", 1))
+    out.append(("small_poisson32_U_P5_flb0", synth.transpose(L), 5, "U", 0))
+    B = synth.banded_lower(1024, seed=3)
+    out.append(("small_banded1024_L_P8", B, 8, "L", 1))
+    out.append(("small_banded1024_U_P3", synth.transpose(B), 3, "U", 1))
+    for seed, m, P, band, dens, far, iso in [
+        (0, 97, 13, 12, 0.4, 0.1, {2, 6, 10, 12}),   # isolated blocks kept split (INF sum wraps)
+        (3, 132, 5, 20, 0.3, 0.0, {4}),               # isolated last block, decision reverted
+        (17, 395, 23, 30, 0.5, 0.01, None),
+        (21, 85, 9, 8, 0.6, 0.0, {0, 1, 6}),          # isolated first blocks
+        (40, 60, 60, 3, 0.9, 0.1, None),              # one row per partition
+    ]:
+        A = rand_upper(m, dens, band, far, seed, iso, P)
+        out.append((f"small_rand{seed}_U_P{P}", A, P, "U", 1))
+    return out
+
+
+def main():
+    if not oracle.Reference.available():
+        raise SystemExit("oracle/_ref/libspike_ref.so is missing: make -C oracle ref")
+    for name, A, P, uplo, flb in small_cases():
+        x_true, b = synth.make_rhs(A, seed=0)
+        st, x = run_reference(A, P, uplo, flb, b)
+        arrays = {f"s_{k}": v for k, v in st.items() if isinstance(v, np.ndarray)}
+        scalars = {f"c_{k}": np.int64(v) for k, v in st.items() if not isinstance(v, np.ndarray)}
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), ia=A.ia, ja=A.ja, a=A.a, b=b, x_ref=x,
+                            meta=np.array([A.m, P, flb, ord(uplo)], dtype=np.int64), **arrays, **scalars)
+        print(name, "saved")
+    dig = {}
+    L = synth.poisson2d_lower(128)
+    big = [("poisson128_L_P4", L, 4, "L", 1), ("poisson128_U_P4", synth.transpose(L), 4, "U", 1)]
+    Bl = synth.banded_lower(65536, seed=0)
+    big += [("banded65536_L_P16", Bl, 16, "L", 1), ("banded65536_L_P64_flb0", Bl, 64, "L", 0),
+            ("banded65536_U_P256", synth.transpose(Bl), 256, "U", 1)]
+    for name, A, P, uplo, flb in big:
+        x_true, b = synth.make_rhs(A, seed=0)
+        st, x = run_reference(A, P, uplo, flb, b)
+        rec = {"m": int(A.m), "nnz": int(A.nnz), "P": P, "uplo": uplo, "flb": flb,
+               "gen": name.split("_")[0], "x_ref_norm": float(np.linalg.norm(x)),
+               "x_ref_err_vs_true": float(np.linalg.norm(x - x_true) / np.linalg.norm(x_true)),
+               "arrays": {k: digest(v) for k, v in st.items() if isinstance(v, np.ndarray)},
+               "sizes": {k: int(v.size) for k, v in st.items() if isinstance(v, np.ndarray)},
+               "scalars": {k: int(v) for k, v in st.items() if not isinstance(v, np.ndarray)}}
+        dig[name] = rec
+        print(name, rec["scalars"])
+    with open(os.path.join(HERE, "digest.json"), "w") as f:
+        json.dump(dig, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,53 @@
+"""C-ABI library: builds, loads without a GPU, exports every symbol the public
+header declares, and refuses to compute without a CUDA device (no CPU fallback)."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import HAS_CUDA, ROOT
+from spike_pstrsv_b200 import build, capi
+
+HEADER = os.path.join(ROOT, "include", "spike_pstrsv.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    funcs = set(re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\**\s*\**([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, flags=re.M))
+    funcs -= {"if", "return"}
+    vars_ = set(re.findall(r"^\s*extern\s+[A-Za-z_ ]+?\s\**([A-Za-z_][A-Za-z0-9_]*)\s*(?:\[|;)", text, flags=re.M))
+    return funcs, vars_
+
+
+def exported():
+    out = subprocess.run(["nm", "-D", "--defined-only", build.LIB], capture_output=True, text=True, check=True)
+    return {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+
+
+def test_library_builds_and_loads():
+    assert os.path.exists(build.build())
+    capi.lib()
+
+
+def test_every_declared_symbol_is_exported():
+    funcs, vars_ = declared_symbols()
+    assert {"spike_pstrsv_preproc", "_spike_pstrsv_preproc", "spike_pstrsv", "spike_pstrsv_solve",
+            "_spike_pstrsv_solve", "free_PSTRSV3", "logPSTRSV3"} <= funcs
+    assert {"PSTRSV_VERBOSE", "FORCE_LOAD_BALANCE", "IS_MATRIX_PARTITIONED", "numRowsReducedSystem",
+            "computeY_timer", "partition_starts"} <= vars_
+    missing = sorted((funcs | vars_) - exported())
+    assert missing == []
+
+
+def test_reference_flag_defaults():
+    assert capi.get_flag("FORCE_LOAD_BALANCE") == 1
+    assert capi.get_flag("PSTRSV_VERBOSE") == 0
+    assert capi.get_flag("IS_MATRIX_PARTITIONED") == 0
+
+
+@pytest.mark.skipif(HAS_CUDA, reason="checks the no-GPU behaviour")
+def test_no_cpu_fallback_without_gpu():
+    with pytest.raises(capi.SpkError):
+        capi.System()
