@@ -74,6 +74,7 @@ extern char PSTRSV_VERBOSE;        /* 1: logPSTRSV3 after preprocessing */
 extern char FORCE_LOAD_BALANCE;    /* 1 (default): optimizeLoadBalance step */
 extern char IS_MATRIX_PARTITIONED; /* 1: use partition_starts/ends as set by the caller, then reset */
 extern char SPK_CLOBBER_B;         /* 1: write the corrected right-hand side back into b */
+extern char SPK_EXACT;             /* 1: no spike truncation (see spk_set_truncation) */
 
 /* Partition bounds (src/spike_pstrsv_globals.h:14-16), sized for SPK_MAX_EXPORTED_PARTS. */
 #define SPK_MAX_EXPORTED_PARTS 65536
@@ -142,6 +143,18 @@ int spk_solve_device(spk_system *s, const double *b, double *x, void *stream);
 
 /* Solve with host or device pointers; synchronous. */
 int spk_solve(spk_system *s, const double *b, double *x);
+
+/* Wait for the system's work and report a device-side failure (a bounded wait
+ * in a kernel that gave up) as SPK_ERR_TIMEOUT. */
+int spk_check(spk_system *s);
+
+/* Spike truncation threshold tau on absolute spike-row sums.  For rows of a
+ * block whose spike row sums to <= tau the coupling correction is at most
+ * tau * ||x||_inf, so the solve keeps the block-local value there, and reduced
+ * rows with sum <= tau are left out of the reduced solve.  Default 2^-60 (below
+ * FP64 resolution); tau < 0 = exact mode (nothing dropped).  Legacy entry
+ * points use 2^-60, or exact mode when SPK_EXACT is set. */
+int spk_set_truncation(spk_system *s, double tau);
 
 /* Structure introspection (reference global names: "ID", "T2", "mapR", "S",
  * "start_intervals", ...): copies up to `capacity` elements to host memory

@@ -58,6 +58,8 @@ def lib() -> ctypes.CDLL:
         L.spk_debug_scalar.restype = ctypes.c_longlong
         L.spk_debug_scalar.argtypes = [vp, ctypes.c_char_p]
         L.spk_legacy_system.restype = vp
+        L.spk_set_truncation.argtypes = [vp, d]
+        L.spk_check.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -135,7 +137,7 @@ def logPSTRSV3(nthreads: int) -> None:
     lib().logPSTRSV3(int(nthreads))
 
 
-_FLAGS = ("PSTRSV_VERBOSE", "FORCE_LOAD_BALANCE", "IS_MATRIX_PARTITIONED", "SPK_CLOBBER_B")
+_FLAGS = ("PSTRSV_VERBOSE", "FORCE_LOAD_BALANCE", "IS_MATRIX_PARTITIONED", "SPK_CLOBBER_B", "SPK_EXACT")
 TIMERS = ("memoryAlloc_timer_pstrsv3", "preprocessD_timer_pstrsv3", "preprocessR_timer_pstrsv3",
           "setDependents_timer_pstrsv3", "preprocessS_timer_pstrsv3",
           "preprocessMappings_timer_pstrsv3", "produceCompressedR_timer_pstrsv3",
@@ -222,6 +224,15 @@ class System:
                                  int(flb), st, en))
         self.n = int(n)
         return self
+
+    def set_truncation(self, tau: float) -> "System":
+        """Spike truncation threshold (default 2^-60); tau < 0 = exact mode."""
+        _check(lib().spk_set_truncation(self.h, float(tau)))
+        return self
+
+    def check(self) -> None:
+        """Wait for the system's stream and raise on a device-side failure."""
+        _check(lib().spk_check(self.h))
 
     def solve(self, b, x=None):
         """Synchronous solve; host (numpy) or device (CUDA tensor) arrays."""

@@ -16,6 +16,7 @@ char PSTRSV_VERBOSE = 0;
 char FORCE_LOAD_BALANCE = 1;
 char IS_MATRIX_PARTITIONED = 0;
 char SPK_CLOBBER_B = 0;
+char SPK_EXACT = 0;
 MKL_INT partition_numRows[SPK_MAX_EXPORTED_PARTS];
 MKL_INT partition_starts[SPK_MAX_EXPORTED_PARTS];
 MKL_INT partition_ends[SPK_MAX_EXPORTED_PARTS];
@@ -151,6 +152,7 @@ void legacy_preproc(double *a, MKL_INT *ia, MKL_INT *ja, int n, int nthreads, ch
     }
     int on_dev = is_device_pointer(a) && is_device_pointer(ia) && is_device_pointer(ja);
     double ph[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    g_legacy->trunc_tol = SPK_EXACT ? -1.0 : kDefaultTruncTol;
     int rc = preprocess(g_legacy, a, ia, ja, n, nthreads, uplo, FORCE_LOAD_BALANCE, starts, ends, on_dev,
                         timed ? ph : nullptr);
     if (rc != SPK_OK) {
@@ -220,6 +222,7 @@ void legacy_solve(char uplo, int m, double *b, double *x, int nthreads, bool tim
     if (rc == SPK_OK && !xd)
         cudaMemcpyAsync(x, dx, sizeof(double) * m, cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
+    if (rc == SPK_OK && e == cudaSuccess) rc = check_device_error(s);
     if (rc != SPK_OK || e != cudaSuccess) {
         if (e != cudaSuccess) set_error(SPK_ERR_CUDA, "solve: %s", cudaGetErrorString(e));
         report("solve");
@@ -357,6 +360,25 @@ int spk_solve(spk_system *s, const double *b, double *x) {
     SPK_TRY(solve(s, db, dx, s->stream, nullptr));
     if (!xd) SPK_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
     SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
+}
+
+int spk_check(spk_system *s) {
+    if (!s) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return check_device_error(s);
+}
+
+int spk_set_truncation(spk_system *s, double tau) {
+    if (!s) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    s->trunc_tol = tau;
+    if (s->built) return solve_prepare(s);
     return SPK_OK;
 }
 
@@ -372,12 +394,16 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "n")) return s->n;
     if (!strcmp(name, "nnz")) return s->nnz;
     if (!strcmp(name, "P")) return s->P;
+    if (!strcmp(name, "rows_phase1")) return s->rows_phase1;
+    if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
+    if (!strcmp(name, "kept_reduced_rows")) return s->nkept;
+    if (!strcmp(name, "reduced_levels")) return s->nlvl;
     if (!strcmp(name, "device_bytes")) {
         long long b = 0;
         b += s->ua.bytes() + s->uia.bytes() + s->uja.bytes() + s->D.bytes() + s->ID.bytes() + s->JD.bytes();
         b += s->T2.bytes() + s->IT2.bytes() + s->JT2.bytes() + s->S.bytes() + s->T.bytes() + s->IT.bytes();
         b += s->JT.bytes() + s->mapR.bytes() + s->dep.bytes() + s->mapRedX.bytes() + s->xbuf.bytes();
-        b += s->red.bytes() + s->rhs_u.bytes() + s->xout_u.bytes();
+        b += s->xout_u.bytes() + s->d_tasks1.bytes() + s->d_tasks2.bytes() + s->d_red_rows.bytes();
         return b;
     }
     return -1;

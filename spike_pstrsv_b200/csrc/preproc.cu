@@ -550,9 +550,13 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         return SPK_ERR_INPUT;
     }
     s->n = n; s->nnz = nnz; s->P = P; s->uplo = up; s->flb = flb;
-    SPK_TRY(s->ua.alloc(nnz));
-    SPK_TRY(s->uia.alloc(n + 1));
-    SPK_TRY(s->uja.alloc(nnz));
+    // padded: the solver stages CSR slices in 16-byte granules that may extend
+    // up to 3 elements past the last nonzero
+    SPK_TRY(s->ua.alloc(nnz + 16));
+    SPK_TRY(s->uia.alloc(n + 16));
+    SPK_TRY(s->uja.alloc(nnz + 16));
+    SPK_CUDA(cudaMemsetAsync(s->ua.p + nnz, 0, 16 * sizeof(double), st));
+    SPK_CUDA(cudaMemsetAsync(s->uja.p + nnz, 0, 16 * sizeof(int), st));
     {
         DBuf<double> la; DBuf<int> lia, lja;
         const double *src_a = a; const int *src_ia = ia, *src_ja = ja;

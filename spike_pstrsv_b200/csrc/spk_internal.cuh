@@ -90,9 +90,18 @@ struct Part {  // per-partition host metadata (reference names in comments)
     int sMapR, eMapR;
 };
 
-struct SolveTask {  // one triangular sweep over rows [lo, hi) of U
+// One warp's job in the segment solver: rows [lo, hi) of U by back
+// substitution, except rows [skip_lo, skip_hi), which take the phase-1 value,
+// and rows [hi, tail), which are copied from the phase-1 values.
+struct SegTask {
     int lo, hi;
+    int skip_lo, skip_hi;
+    int tail;
 };
+
+// Truncation threshold on absolute spike-row sums (2^-60, below FP64 resolution
+// relative to ||x||_inf); negative = exact mode (nothing dropped).
+constexpr double kDefaultTruncTol = 8.673617379884035e-19;
 
 }  // namespace spk
 
@@ -116,13 +125,14 @@ struct spk_system {
     spk::DBuf<double> D, T2, S, T;
     spk::DBuf<int> ID, JD, IT2, JT2, mapR, dep, mapRedX, IT, JT;
     // solve support
+    double trunc_tol = spk::kDefaultTruncTol;
     spk::DBuf<int> d_ps, d_pe, d_lvl;  // partition bounds; reduced row offset per partition
-    spk::DBuf<spk::SolveTask> d_tasks1, d_tasks2, d_copy2;
-    int ntasks1 = 0, ntasks2 = 0, ncopy2 = 0;
-    spk::DBuf<double> xbuf, red, rhs_u, xout_u;
-    std::vector<int> lvl_nonempty;  // partitions (descending) whose reduced rows hold entries
-    spk::DBuf<int> d_lvl_list;
-    int nlvl = 0;
+    spk::DBuf<spk::SegTask> d_tasks1, d_tasks2;
+    int ntasks1 = 0, ntasks2 = 0;
+    long long rows_phase1 = 0, rows_phase4 = 0;  // rows solved per call by phase 1 / phase 4
+    spk::DBuf<double> xbuf, xout_u;
+    spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
+    int nlvl = 0, nkept = 0;
     cudaStream_t stream = nullptr;
     int own_stream = 0;
 };
@@ -134,6 +144,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
                double *phase_seconds);
 int solve(spk_system *s, const double *b, double *x, cudaStream_t stream, double *phase_seconds);
 int solve_prepare(spk_system *s);
+int check_device_error(spk_system *s);
 
 // pointer classification
 int is_device_pointer(const void *p);

@@ -212,3 +212,27 @@ def test_full_size_banded_lower(P):
         bad = [k for k, h in rec["arrays"].items() if sha(got[k]) != h]
         bad += [k for k, v in rec["scalars"].items() if int(got[k]) != v]
         assert bad == []
+
+
+@pytest.mark.parametrize("path", SMALL[:6], ids=[os.path.basename(p)[6:-4] for p in SMALL[:6]])
+def test_gpu_exact_mode_matches_golden(path):
+    A, P, flb, uplo, b, x_ref, want = load_small(path)
+    S = gpu_system(A, P, uplo, flb).set_truncation(-1.0)
+    assert S.scalar("rows_phase4") >= 0
+    assert rel_err(S.solve(b), x_ref) <= TOL
+
+
+def test_truncation_engages_on_decaying_spikes_and_stays_accurate():
+    L = synth.banded_lower(262144, seed=9)
+    x_true, b = synth.make_rhs(L, seed=9)
+    xs = oracle.sequential_solve(L, b, "L")
+    S = gpu_system(L, 64, "L", 1)
+    assert S.scalar("rows_phase4") < L.m // 2      # D2 work cut to the coupled rows
+    assert S.scalar("kept_reduced_rows") == 0       # every reduced row below 2^-60
+    x = S.solve(b)
+    assert rel_err(x, xs) <= TOL
+    E = gpu_system(L, 64, "L", 1).set_truncation(-1.0)
+    assert E.scalar("rows_phase4") > L.m // 2
+    xe = E.solve(b)
+    assert rel_err(xe, xs) <= TOL
+    assert rel_err(x, xe) <= 1e-15
