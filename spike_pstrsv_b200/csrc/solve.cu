@@ -42,7 +42,7 @@ constexpr int kWin = 128;       // rows of recently solved x kept in shared memo
 constexpr int kCap = 640;       // staged nonzeros per tile (32 rows); larger tiles read global memory
 constexpr int kCapV = kCap + 2; // + alignment slack (16-byte granules of doubles)
 constexpr int kCapC = kCap + 8; // + alignment slack (16-byte granules of ints)
-constexpr unsigned kSpinLimit = 1u << 26;
+constexpr long long kWaitCycles = 1ll << 32;  // ~2 s at B200 clocks: bound of every barrier wait
 
 inline double now_s() {
     timespec ts;
@@ -186,9 +186,9 @@ __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int l
         // wait for this tile's slice
         const bool direct = cur.direct;
         if (!direct) {
-            unsigned spins = 0;
+            const long long t0 = clock64();
             while (!mbar_try_wait(&S.bar[slot], (phase >> slot) & 1u)) {
-                if (++spins > kSpinLimit) {
+                if (clock64() - t0 > kWaitCycles) {
                     if (lane == 0) atomicExch(A.err, 1);
                     return false;
                 }
