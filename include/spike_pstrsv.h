@@ -156,6 +156,13 @@ int spk_check(spk_system *s);
  * points use 2^-60, or exact mode when SPK_EXACT is set. */
 int spk_set_truncation(spk_system *s, double tau);
 
+/* Per-phase device timing with CUDA events recorded on the solve's stream:
+ * spk_set_profiling(s, 1) enables it; spk_phase_times returns (and resets) the
+ * accumulated milliseconds of phase 1 (block-local D1 solves), phase 2 (reduced
+ * system) and phase 3+4 (coupled D2/D solves) and the number of solves timed. */
+int spk_set_profiling(spk_system *s, int on);
+int spk_phase_times(spk_system *s, double *ms3, long long *solves);
+
 /* Structure introspection (reference global names: "ID", "T2", "mapR", "S",
  * "start_intervals", ...): copies up to `capacity` elements to host memory
  * `dst` and stores the full element count and type code ('d' double, 'i'

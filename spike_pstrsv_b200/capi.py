@@ -60,6 +60,8 @@ def lib() -> ctypes.CDLL:
         L.spk_legacy_system.restype = vp
         L.spk_set_truncation.argtypes = [vp, d]
         L.spk_check.argtypes = [vp]
+        L.spk_set_profiling.argtypes = [vp, i]
+        L.spk_phase_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
     return _lib
 
@@ -229,6 +231,17 @@ class System:
         """Spike truncation threshold (default 2^-60); tau < 0 = exact mode."""
         _check(lib().spk_set_truncation(self.h, float(tau)))
         return self
+
+    def set_profiling(self, on: bool = True) -> "System":
+        _check(lib().spk_set_profiling(self.h, int(on)))
+        return self
+
+    def phase_times(self):
+        """(ms of phase 1, phase 2, phase 3+4 accumulated, number of solves); resets."""
+        ms = (ctypes.c_double * 3)()
+        n = ctypes.c_longlong()
+        _check(lib().spk_phase_times(self.h, ms, ctypes.byref(n)))
+        return [ms[0], ms[1], ms[2]], n.value
 
     def check(self) -> None:
         """Wait for the system's stream and raise on a device-side failure."""

@@ -99,6 +99,9 @@ int make_system(spk_system **out) {
 void destroy_system(spk_system *s) {
     if (!s) return;
     if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto &set : s->ev)
+        for (auto &e : set)
+            if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -372,6 +375,33 @@ int spk_check(spk_system *s) {
     return check_device_error(s);
 }
 
+int spk_set_profiling(spk_system *s, int on) {
+    if (!s) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (on && !s->ev[0][0])
+        for (auto &set : s->ev)
+            for (auto &e : set) SPK_CUDA(cudaEventCreate(&e));
+    s->profiling = on;
+    return SPK_OK;
+}
+
+int spk_phase_times(spk_system *s, double *ms3, long long *solves) {
+    if (!s || !ms3) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    SPK_TRY(collect_phase_times(s));
+    for (int k = 0; k < 3; k++) {
+        ms3[k] = s->phase_ms[k];
+        s->phase_ms[k] = 0;
+    }
+    if (solves) *solves = s->profiled_solves;
+    s->profiled_solves = 0;
+    return SPK_OK;
+}
+
 int spk_set_truncation(spk_system *s, double tau) {
     if (!s) {
         set_error(SPK_ERR_ARG, "null argument");
@@ -395,6 +425,8 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "nnz")) return s->nnz;
     if (!strcmp(name, "P")) return s->P;
     if (!strcmp(name, "rows_phase1")) return s->rows_phase1;
+    if (!strcmp(name, "launches")) return s->launches;
+    if (!strcmp(name, "launches_per_solve")) return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
     if (!strcmp(name, "kept_reduced_rows")) return s->nkept;
     if (!strcmp(name, "reduced_levels")) return s->nlvl;

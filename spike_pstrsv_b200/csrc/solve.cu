@@ -105,7 +105,8 @@ struct TileStage {
 struct SegSmem {
     alignas(16) double v[2][kCapV];
     alignas(16) int c[2][kCapC];
-    alignas(16) double coef[32][32];  // [tile column][lane row]
+    alignas(16) double coef[32][32];  // [tile column i][lane row l] = a(l, i) / a(i, i)
+    double rdv[32];                   // 1 / diagonal of the tile's rows
     double win[kWin];                 // x of the last kWin solved rows, by row mod kWin
     alignas(8) unsigned long long bar[2];
 };
@@ -140,6 +141,17 @@ __device__ __forceinline__ void stage_tile(const SegArgs &A, SegSmem &S, int slo
     mbar_arrive_expect_tx(&S.bar[slot], bv + bc);
     bulk_g2s(S.v[slot], A.a + ts.s0v, bv, &S.bar[slot]);
     bulk_g2s(S.c[slot], A.ja + ts.s0c, bc, &S.bar[slot]);
+}
+
+// x at a column below the current tile: solved in this task (shared window or
+// xout) when c < hi_ext; else the fixed phase 1-2 value (FULL) or nothing (!FULL).
+template <bool FULL>
+__device__ __forceinline__ double solved_x(const SegArgs &A, const SegSmem &S, int c, int top, int hi_ext) {
+    if (c < hi_ext) {
+        if (c < top + kWin) return S.win[c & (kWin - 1)];
+        return A.xout[A.rev_out ? A.n - 1 - c : c];
+    }
+    return FULL ? A.xfix[c] : 0.0;
 }
 
 // Solve rows [lo, hi) of the task bottom-up.  Columns >= hi_ext take xfix
@@ -180,9 +192,6 @@ __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int l
             const int r = max(lo, r0 - 32) + lane;
             rhs_next = (r < r0) ? A.rhs[A.rev_in ? n - 1 - r : r] : 0.0;
         }
-        // clear the coefficient tile
-#pragma unroll
-        for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
         // wait for this tile's slice
         const bool direct = cur.direct;
         if (!direct) {
@@ -199,38 +208,53 @@ __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int l
         const double *vb = direct ? A.a : S.v[slot];
         const int *cb = direct ? A.ja : S.c[slot];
         const int ov = direct ? 0 : cur.s0v, oc = direct ? 0 : cur.s0c;
+        // row bounds, diagonal reciprocal and right-hand side
+        int b = 0, e = 0;
         double acc = 0.0, rd = 0.0;
         if (lane < nr) {
             const int r = r0 + lane;
-            const int b = A.ia[r], e = A.ia[r + 1];
-            acc = rhs_cur;
+            b = A.ia[r];
+            e = A.ia[r + 1];
             rd = 1.0 / vb[b - ov];
-            for (int q = b + 1; q < e; q++) {
-                const int c = cb[q - oc];
-                const double v = vb[q - ov];
-                if (c < top) {
-                    S.coef[c - r0][lane] = v;
-                } else if (c < hi_ext) {
-                    double xc;
-                    if (c < top + kWin) xc = S.win[c & (kWin - 1)];
-                    else xc = A.xout[A.rev_out ? n - 1 - c : c];
-                    acc = fma(-v, xc, acc);
-                } else if (FULL) {
-                    acc = fma(-v, A.xfix[c], acc);
-                }
-            }
+            acc = rhs_cur;
         }
+        S.rdv[lane] = rd;
         __syncwarp();
+        // in-tile entries (columns r < c < top come first in the sorted row):
+        // coefficient a(r, c) / a(c, c) into column c - r0 of the tile
+        int q = b + 1;
+        for (; q < e; q++) {
+            const int c = cb[q - oc];
+            if (c >= top) break;
+            S.coef[c - r0][lane] = vb[q - ov] * S.rdv[c - r0];
+        }
+        const int q_in_end = q;
+        // entries at solved rows below the tile, four independent partial sums
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+        for (; q + 3 < e; q += 4) {
+            const int c0 = cb[q - oc], c1 = cb[q + 1 - oc], c2 = cb[q + 2 - oc], c3 = cb[q + 3 - oc];
+            const double v0 = vb[q - ov], v1 = vb[q + 1 - ov], v2 = vb[q + 2 - ov], v3 = vb[q + 3 - ov];
+            p0 = fma(v0, solved_x<FULL>(A, S, c0, top, hi_ext), p0);
+            p1 = fma(v1, solved_x<FULL>(A, S, c1, top, hi_ext), p1);
+            p2 = fma(v2, solved_x<FULL>(A, S, c2, top, hi_ext), p2);
+            p3 = fma(v3, solved_x<FULL>(A, S, c3, top, hi_ext), p3);
+        }
+        for (; q < e; q++) p0 = fma(vb[q - ov], solved_x<FULL>(A, S, cb[q - oc], top, hi_ext), p0);
+        acc -= (p0 + p1) + (p2 + p3);
+        __syncwarp();
+        // in-tile triangle: step i broadcasts lane i's final accumulator
         double myx = 0.0;
 #pragma unroll
         for (int i = 31; i >= 0; i--) {
             if (i < nr) {
                 const double ci = S.coef[i][lane];
-                const double xi = __shfl_sync(0xffffffffu, acc * rd, i);
-                if (lane == i) myx = xi;
-                acc = fma(-ci, xi, acc);
+                const double ai = __shfl_sync(0xffffffffu, acc, i);
+                if (lane == i) myx = ai * rd;
+                acc = fma(-ci, ai, acc);
             }
         }
+        // leave the coefficient tile zero for the next tile
+        for (int q2 = b + 1; q2 < q_in_end; q2++) S.coef[cb[q2 - oc] - r0][lane] = 0.0;
         if (lane < nr) {
             const int r = r0 + lane;
             A.xout[A.rev_out ? n - 1 - r : r] = myx;
@@ -264,6 +288,8 @@ __global__ void __launch_bounds__(32) k_segment_solve(SegArgs A) {
         mbar_init(&S.bar[1], 1);
         fence_mbar_init();
     }
+#pragma unroll
+    for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
     __syncwarp();
     unsigned phase = 0u;  // bit k: parity of the next completion of stage k
     const SegTask t = A.tasks[task];
@@ -476,6 +502,12 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
     };
     if (ph) { cudaStreamSynchronize(st); t0 = now_s(); }
     lap(0);
+    const bool prof = s->profiling && s->ev[0][0];
+    const int ring = (int)(s->ev_next % spk_system::kEvRing);
+    if (prof) {
+        if (s->ev_pending[ring]) SPK_TRY(collect_event_set(s, ring));
+        cudaEventRecord(s->ev[ring][0], st);
+    }
     SegArgs A;
     A.ia = s->uia.p;
     A.ja = s->uja.p;
@@ -492,13 +524,17 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         A.rev_out = 0;
         k_segment_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
         SPK_CUDA(cudaGetLastError());
+        s->launches++;
     }
+    if (prof) cudaEventRecord(s->ev[ring][1], st);
     lap(1);
     if (s->redNec && s->nkept) {
         k_reduced_solve<<<1, 1024, 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p, s->IT.p,
                                             s->JT.p, s->T.p, s->xbuf.p);
         SPK_CUDA(cudaGetLastError());
+        s->launches++;
     }
+    if (prof) cudaEventRecord(s->ev[ring][2], st);
     lap(2);
     A.tasks = s->d_tasks2.p;
     A.ntasks = s->ntasks2;
@@ -507,7 +543,31 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
     A.rev_out = s->uplo == 'L';
     k_segment_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
     SPK_CUDA(cudaGetLastError());
+    s->launches++;
+    if (prof) {
+        cudaEventRecord(s->ev[ring][3], st);
+        s->ev_pending[ring] = 1;
+        s->ev_next++;
+    }
     lap(3);
+    return SPK_OK;
+}
+
+int collect_event_set(spk_system *s, int k) {
+    SPK_CUDA(cudaEventSynchronize(s->ev[k][3]));
+    for (int p = 0; p < 3; p++) {
+        float ms = 0;
+        SPK_CUDA(cudaEventElapsedTime(&ms, s->ev[k][p], s->ev[k][p + 1]));
+        s->phase_ms[p] += ms;
+    }
+    s->ev_pending[k] = 0;
+    s->profiled_solves++;
+    return SPK_OK;
+}
+
+int collect_phase_times(spk_system *s) {
+    for (int k = 0; k < spk_system::kEvRing; k++)
+        if (s->ev_pending[k]) SPK_TRY(collect_event_set(s, k));
     return SPK_OK;
 }
 

@@ -133,6 +133,14 @@ struct spk_system {
     spk::DBuf<double> xbuf, xout_u;
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
+    // optional per-phase device timing (spk_set_profiling)
+    int profiling = 0;
+    static constexpr int kEvRing = 64;           // event sets in flight before a forced collection
+    cudaEvent_t ev[kEvRing][4] = {};
+    int ev_pending[kEvRing] = {};
+    long long ev_next = 0;
+    double phase_ms[3] = {0, 0, 0};
+    long long profiled_solves = 0, launches = 0;
     cudaStream_t stream = nullptr;
     int own_stream = 0;
 };
@@ -145,6 +153,8 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
 int solve(spk_system *s, const double *b, double *x, cudaStream_t stream, double *phase_seconds);
 int solve_prepare(spk_system *s);
 int check_device_error(spk_system *s);
+int collect_phase_times(spk_system *s);
+int collect_event_set(spk_system *s, int k);
 
 // pointer classification
 int is_device_pointer(const void *p);
