@@ -426,6 +426,8 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "P")) return s->P;
     if (!strcmp(name, "rows_phase1")) return s->rows_phase1;
     if (!strcmp(name, "launches")) return s->launches;
+    if (!strcmp(name, "ell")) return s->ell_ok;
+    if (!strcmp(name, "ell_entries")) return s->ell_entries;
     if (!strcmp(name, "launches_per_solve")) return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
     if (!strcmp(name, "kept_reduced_rows")) return s->nkept;
@@ -436,6 +438,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->T2.bytes() + s->IT2.bytes() + s->JT2.bytes() + s->S.bytes() + s->T.bytes() + s->IT.bytes();
         b += s->JT.bytes() + s->mapR.bytes() + s->dep.bytes() + s->mapRedX.bytes() + s->xbuf.bytes();
         b += s->xout_u.bytes() + s->d_tasks1.bytes() + s->d_tasks2.bytes() + s->d_red_rows.bytes();
+        b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
         return b;
     }
     return -1;

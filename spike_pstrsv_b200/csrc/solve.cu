@@ -30,6 +30,7 @@
 // the solution stores.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <ctime>
 
 #include "spk_internal.cuh"
@@ -97,16 +98,18 @@ __device__ __forceinline__ void fence_mbar_init() {
 
 // ---- segment solver -------------------------------------------------------------
 
+constexpr int kCapR = 34;        // staged 1/diagonal values per tile (+ alignment slack)
+
 struct TileStage {
-    int s0v, s0c;   // first staged value / column element (aligned down)
-    int direct;     // 1: tile read from global memory (too many nonzeros to stage)
+    int s0v, s0c, s0r;  // first staged value / column / reciprocal element (aligned down)
+    int direct;         // 1: values and columns read from global memory (too many nonzeros)
 };
 
 struct SegSmem {
     alignas(16) double v[2][kCapV];
     alignas(16) int c[2][kCapC];
+    alignas(16) double rd[2][kCapR];  // 1 / diagonal of the tile's rows
     alignas(16) double coef[32][32];  // [tile column i][lane row l] = a(l, i) / a(i, i)
-    double rdv[32];                   // 1 / diagonal of the tile's rows
     double win[kWin];                 // x of the last kWin solved rows, by row mod kWin
     alignas(8) unsigned long long bar[2];
 };
@@ -117,30 +120,48 @@ struct SegArgs {
     const int *ia;
     const int *ja;
     const double *a;
+    const double *rdiag;  // 1 / diagonal per row of U (padded for 16-byte granules)
+    const double *ell_val;  // sliced ELL of U's off-diagonals over absolute 32-row tiles
+    const int *ell_col;
+    const int *ell_ptr;     // tile j occupies entries [ell_ptr[j], ell_ptr[j+1]); slot k of row 32j+l at +32k+l
     int n;
-    const double *rhs;   // right-hand side in the caller's order
-    const double *xfix;  // U-order x of phases 1-2 (FULL mode)
-    double *xout;        // output
-    int rev_in;          // rhs[i] holds row n-1-i of U
-    int rev_out;         // xout is stored in the caller's order with reversal
+    const double *rhs;    // right-hand side in the caller's order
+    const double *xfix;   // U-order x of phases 1-2 (FULL mode)
+    double *xout;         // output
+    int rev_in;           // rhs[i] holds row n-1-i of U
+    int rev_out;          // xout is stored in the caller's order with reversal
     int *err;
 };
 
-// Issue (lane 0) the bulk copies staging tile [r0, top): values and columns of
-// nonzeros ia[r0] .. ia[top], widened to 16-byte granules.
-__device__ __forceinline__ void stage_tile(const SegArgs &A, SegSmem &S, int slot, int r0, int top,
-                                           TileStage &ts) {
-    const int e0 = A.ia[r0], e1 = A.ia[top];
+// Lane 0: stage tile [r0, top) whose nonzeros are [e0, e1): the reciprocals of
+// its diagonal and, unless the tile is too large, its values and column
+// indices, each widened to 16-byte granules.
+__device__ __forceinline__ void stage_tile(const SegArgs &A, SegSmem &S, int slot, int r0, int top, int e0,
+                                           int e1, TileStage &ts) {
     ts.direct = (e1 - e0) > kCap;
     ts.s0v = e0 & ~1;
     ts.s0c = e0 & ~3;
-    if (ts.direct) return;
-    const int endv = (e1 + 1) & ~1, endc = (e1 + 3) & ~3;
-    const unsigned bv = (unsigned)(endv - ts.s0v) * 8u, bc = (unsigned)(endc - ts.s0c) * 4u;
+    ts.s0r = r0 & ~1;
+    const unsigned br = (unsigned)(((top + 1) & ~1) - ts.s0r) * 8u;
+    unsigned bv = 0, bc = 0;
+    if (!ts.direct) {
+        bv = (unsigned)(((e1 + 1) & ~1) - ts.s0v) * 8u;
+        bc = (unsigned)(((e1 + 3) & ~3) - ts.s0c) * 4u;
+    }
     fence_proxy_async();
-    mbar_arrive_expect_tx(&S.bar[slot], bv + bc);
-    bulk_g2s(S.v[slot], A.a + ts.s0v, bv, &S.bar[slot]);
-    bulk_g2s(S.c[slot], A.ja + ts.s0c, bc, &S.bar[slot]);
+    mbar_arrive_expect_tx(&S.bar[slot], br + bv + bc);
+    bulk_g2s(S.rd[slot], A.rdiag + ts.s0r, br, &S.bar[slot]);
+    if (!ts.direct) {
+        bulk_g2s(S.v[slot], A.a + ts.s0v, bv, &S.bar[slot]);
+        bulk_g2s(S.c[slot], A.ja + ts.s0c, bc, &S.bar[slot]);
+    }
+}
+
+__device__ __forceinline__ void bcast_stage(TileStage &t) {
+    t.direct = __shfl_sync(0xffffffffu, t.direct, 0);
+    t.s0v = __shfl_sync(0xffffffffu, t.s0v, 0);
+    t.s0c = __shfl_sync(0xffffffffu, t.s0c, 0);
+    t.s0r = __shfl_sync(0xffffffffu, t.s0r, 0);
 }
 
 // x at a column below the current tile: solved in this task (shared window or
@@ -156,45 +177,65 @@ __device__ __forceinline__ double solved_x(const SegArgs &A, const SegSmem &S, i
 
 // Solve rows [lo, hi) of the task bottom-up.  Columns >= hi_ext take xfix
 // (FULL) or are skipped (!FULL).  Solved rows are written to xout and to the
-// shared window.  Returns false after a timed-out wait.
+// shared window.  Row pointers are prefetched two tiles ahead and the
+// right-hand side one tile ahead, in registers; the tile's CSR slice and
+// diagonal reciprocals are staged one tile ahead by the bulk-copy engine.
+// Returns false after a timed-out wait.
 template <bool FULL>
 __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int lo, int hi, int hi_ext) {
+    const unsigned FULLMASK = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     if (hi <= lo) return true;
-    const int ntiles = (hi - lo + 31) / 32;
-    TileStage cur;
-    if (lane == 0) stage_tile(A, S, 0, max(lo, hi - 32), hi, cur);
-    cur.direct = __shfl_sync(0xffffffffu, cur.direct, 0);
-    cur.s0v = __shfl_sync(0xffffffffu, cur.s0v, 0);
-    cur.s0c = __shfl_sync(0xffffffffu, cur.s0c, 0);
     const int n = A.n;
-    // right-hand side of the first tile
-    double rhs_next = 0.0;
+    const int ntiles = (hi - lo + 31) / 32;
+    // tile k covers rows [r0_k, top_k): top_0 = hi, top_{k+1} = r0_k, r0_k = max(lo, top_k - 32)
+    int top = hi, r0 = max(lo, hi - 32);
+    int top1 = r0, r01 = max(lo, r0 - 32);
+    auto load_ia = [&](int rr0, int rtop) {
+        const int r = rr0 + lane;
+        return A.ia[r < rtop ? r : rtop];
+    };
+    auto load_rhs = [&](int rr0, int rtop) {
+        const int r = rr0 + lane;
+        return r < rtop ? A.rhs[A.rev_in ? n - 1 - r : r] : 0.0;
+    };
+    int ia_top = A.ia[hi];                                 // ia[top] of the current tile
+    int ia_c = load_ia(r0, top);                           // ia[r0 + lane] of the current tile
+    int ia_n = ntiles > 1 ? load_ia(r01, top1) : 0;        // the next tile's
+    double rhs_c = load_rhs(r0, top);
+    TileStage cur;
     {
-        const int r = max(lo, hi - 32) + lane;
-        if (r < hi) rhs_next = A.rhs[A.rev_in ? n - 1 - r : r];
+        const int e0 = __shfl_sync(FULLMASK, ia_c, 0);
+        if (lane == 0) stage_tile(A, S, 0, r0, top, e0, ia_top, cur);
+        bcast_stage(cur);
     }
     for (int it = 0; it < ntiles; it++) {
-        const int top = hi - 32 * it;
-        const int r0 = max(lo, top - 32), nr = top - r0;
         const int slot = it & 1;
-        // stage the next tile (its slot was released at the end of tile it-1)
+        const int nr = top - r0;
+        // prefetch: right-hand side of tile it+1, row pointers of tile it+2;
+        // stage tile it+1 (its slot was released at the end of tile it-1)
+        int top2 = 0, r02 = 0, ia_nn = 0;
+        double rhs_n = 0.0;
         TileStage nxt = cur;
         if (it + 1 < ntiles) {
-            const int top1 = r0, r01 = max(lo, top1 - 32);
-            if (lane == 0) stage_tile(A, S, slot ^ 1, r01, top1, nxt);
-            nxt.direct = __shfl_sync(0xffffffffu, nxt.direct, 0);
-            nxt.s0v = __shfl_sync(0xffffffffu, nxt.s0v, 0);
-            nxt.s0c = __shfl_sync(0xffffffffu, nxt.s0c, 0);
+            rhs_n = load_rhs(r01, top1);
+            if (it + 2 < ntiles) {
+                top2 = r01;
+                r02 = max(lo, r01 - 32);
+                ia_nn = load_ia(r02, top2);
+            }
+            const int e0 = __shfl_sync(FULLMASK, ia_n, 0);
+            const int e1 = __shfl_sync(FULLMASK, ia_c, 0);  // ia[top1] = ia[r0]
+            if (lane == 0) stage_tile(A, S, slot ^ 1, r01, top1, e0, e1, nxt);
+            bcast_stage(nxt);
         }
-        const double rhs_cur = rhs_next;
-        if (it + 1 < ntiles) {
-            const int r = max(lo, r0 - 32) + lane;
-            rhs_next = (r < r0) ? A.rhs[A.rev_in ? n - 1 - r : r] : 0.0;
-        }
+        // row bounds of this tile
+        int b = ia_c;
+        int e = __shfl_down_sync(FULLMASK, ia_c, 1);
+        if (lane == nr - 1) e = ia_top;
+        if (lane >= nr) b = e = 0;
         // wait for this tile's slice
-        const bool direct = cur.direct;
-        if (!direct) {
+        {
             const long long t0 = clock64();
             while (!mbar_try_wait(&S.bar[slot], (phase >> slot) & 1u)) {
                 if (clock64() - t0 > kWaitCycles) {
@@ -204,63 +245,75 @@ __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int l
             }
             phase ^= 1u << slot;
         }
-        __syncwarp();
+        const bool direct = cur.direct;
         const double *vb = direct ? A.a : S.v[slot];
         const int *cb = direct ? A.ja : S.c[slot];
         const int ov = direct ? 0 : cur.s0v, oc = direct ? 0 : cur.s0c;
-        // row bounds, diagonal reciprocal and right-hand side
-        int b = 0, e = 0;
-        double acc = 0.0, rd = 0.0;
-        if (lane < nr) {
-            const int r = r0 + lane;
-            b = A.ia[r];
-            e = A.ia[r + 1];
-            rd = 1.0 / vb[b - ov];
-            acc = rhs_cur;
-        }
-        S.rdv[lane] = rd;
-        __syncwarp();
-        // in-tile entries (columns r < c < top come first in the sorted row):
-        // coefficient a(r, c) / a(c, c) into column c - r0 of the tile
-        int q = b + 1;
-        for (; q < e; q++) {
-            const int c = cb[q - oc];
-            if (c >= top) break;
-            S.coef[c - r0][lane] = vb[q - ov] * S.rdv[c - r0];
-        }
-        const int q_in_end = q;
-        // entries at solved rows below the tile, four independent partial sums
-        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
-        for (; q + 3 < e; q += 4) {
-            const int c0 = cb[q - oc], c1 = cb[q + 1 - oc], c2 = cb[q + 2 - oc], c3 = cb[q + 3 - oc];
-            const double v0 = vb[q - ov], v1 = vb[q + 1 - ov], v2 = vb[q + 2 - ov], v3 = vb[q + 3 - ov];
-            p0 = fma(v0, solved_x<FULL>(A, S, c0, top, hi_ext), p0);
-            p1 = fma(v1, solved_x<FULL>(A, S, c1, top, hi_ext), p1);
-            p2 = fma(v2, solved_x<FULL>(A, S, c2, top, hi_ext), p2);
-            p3 = fma(v3, solved_x<FULL>(A, S, c3, top, hi_ext), p3);
-        }
-        for (; q < e; q++) p0 = fma(vb[q - ov], solved_x<FULL>(A, S, cb[q - oc], top, hi_ext), p0);
-        acc -= (p0 + p1) + (p2 + p3);
-        __syncwarp();
-        // in-tile triangle: step i broadcasts lane i's final accumulator
-        double myx = 0.0;
+        const double *rdt = S.rd[slot] - 0;
+        const int orr = cur.s0r;
+        const double rd = lane < nr ? rdt[r0 + lane - orr] : 0.0;
+        double acc = rhs_c;
+        // entries after the diagonal: in-tile columns (r < c < top) give the
+        // coefficient a(r, c) / a(c, c); solved columns below the tile are summed
+        double p[4] = {0.0, 0.0, 0.0, 0.0};
+        unsigned mask = 0u;
+        for (int q = b + 1; q < e; q += 4) {
 #pragma unroll
-        for (int i = 31; i >= 0; i--) {
-            if (i < nr) {
+            for (int k = 0; k < 4; k++) {
+                const int qq = q + k;
+                if (qq < e) {
+                    const int c = cb[qq - oc];
+                    const double v = vb[qq - ov];
+                    if (c < top) {
+                        S.coef[c - r0][lane] = v * rdt[c - orr];
+                        mask |= 1u << (c - r0);
+                    } else {
+                        p[k] = fma(v, solved_x<FULL>(A, S, c, top, hi_ext), p[k]);
+                    }
+                }
+            }
+        }
+        acc -= (p[0] + p[1]) + (p[2] + p[3]);
+        __syncwarp();
+        // in-tile triangle: step i broadcasts lane i's (final) accumulator.  Lane
+        // i's row has no entries left of its diagonal, so its accumulator does
+        // not change after its own step.
+        if (nr == 32) {
+#pragma unroll
+            for (int i = 31; i >= 0; i--) {
                 const double ci = S.coef[i][lane];
-                const double ai = __shfl_sync(0xffffffffu, acc, i);
-                if (lane == i) myx = ai * rd;
+                const double ai = __shfl_sync(FULLMASK, acc, i);
+                acc = fma(-ci, ai, acc);
+            }
+        } else {
+            for (int i = nr - 1; i >= 0; i--) {
+                const double ci = S.coef[i][lane];
+                const double ai = __shfl_sync(FULLMASK, acc, i);
                 acc = fma(-ci, ai, acc);
             }
         }
+        const double myx = acc * rd;
         // leave the coefficient tile zero for the next tile
-        for (int q2 = b + 1; q2 < q_in_end; q2++) S.coef[cb[q2 - oc] - r0][lane] = 0.0;
+        while (mask) {
+            const int i = __ffs(mask) - 1;
+            S.coef[i][lane] = 0.0;
+            mask &= mask - 1u;
+        }
         if (lane < nr) {
             const int r = r0 + lane;
             A.xout[A.rev_out ? n - 1 - r : r] = myx;
             S.win[r & (kWin - 1)] = myx;
         }
         __syncwarp();
+        // advance
+        ia_top = __shfl_sync(FULLMASK, ia_c, 0);
+        ia_c = ia_n;
+        ia_n = ia_nn;
+        rhs_c = rhs_n;
+        top = top1;
+        r0 = r01;
+        top1 = top2;
+        r01 = r02;
         cur = nxt;
     }
     return true;
@@ -302,6 +355,236 @@ __global__ void __launch_bounds__(32) k_segment_solve(SegArgs A) {
     } else {
         solve_range<FULL>(A, S, phase, t.lo, t.hi, t.hi);
     }
+}
+
+// ---- tile solver on the sliced-ELL layout -----------------------------------------
+//
+// Same algorithm as the CSR segment solver, on absolute 32-row tiles: tile j =
+// rows [32j, 32j+32); a task covers its tiles from the one holding hi-1 down to
+// the one holding lo, with the rows outside [lo, hi) masked.  The tile's slots
+// are contiguous (32 x width values and columns, 128/256-byte aligned), so each
+// tile is one pair of bulk copies with no alignment slack, lanes read their
+// slots conflict-free, and every lane runs the same number of slot steps.
+
+constexpr int kEllCap = 20;  // staged slots per row; wider tiles are read from global memory
+
+struct TileSmem {
+    alignas(128) double v[2][kEllCap * 32];
+    alignas(128) int c[2][kEllCap * 32];
+    alignas(128) double rd[2][32];     // 1 / diagonal of the tile's rows
+    alignas(16) double coef[32][32];   // [tile column i][lane row l] = a(l, i) / a(i, i)
+    double win[kWin];                  // x of the last kWin solved rows, by row mod kWin
+    alignas(8) unsigned long long bar[2];
+};
+
+// Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and, when it
+// is at most kEllCap slots wide, its values and columns.
+__device__ __forceinline__ void stage_ell(const SegArgs &A, TileSmem &S, int slot, int j, int e0, int e1) {
+    const unsigned ne = (unsigned)(e1 - e0);
+    const bool staged = ne <= (unsigned)(kEllCap * 32);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&S.bar[slot], 256u + (staged ? ne * 12u : 0u));
+    bulk_g2s(S.rd[slot], A.rdiag + 32ll * j, 256u, &S.bar[slot]);
+    if (staged && ne) {
+        bulk_g2s(S.v[slot], A.ell_val + e0, ne * 8u, &S.bar[slot]);
+        bulk_g2s(S.c[slot], A.ell_col + e0, ne * 4u, &S.bar[slot]);
+    }
+}
+
+template <bool FULL>
+__device__ __forceinline__ double tile_solved_x(const SegArgs &A, const TileSmem &S, int c, int top, int hi_ext) {
+    if (c < hi_ext) {
+        if (c < top + kWin) return S.win[c & (kWin - 1)];
+        return A.xout[A.rev_out ? A.n - 1 - c : c];
+    }
+    return FULL ? A.xfix[c] : 0.0;
+}
+
+template <bool FULL>
+__device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int lo, int hi, int hi_ext) {
+    const unsigned FULLMASK = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (hi <= lo) return true;
+    const int n = A.n;
+    const int jt = (hi - 1) >> 5, jb = lo >> 5;
+    const int ntiles = jt - jb + 1;
+    auto load_rhs = [&](int j) {
+        const int r = 32 * j + lane;
+        return (r >= lo && r < hi) ? A.rhs[A.rev_in ? n - 1 - r : r] : 0.0;
+    };
+    int p_hi = A.ell_ptr[jt + 1], p_lo = A.ell_ptr[jt];
+    int p_next = ntiles > 1 ? A.ell_ptr[jt - 1] : 0;
+    double rhs_c = load_rhs(jt);
+    if (lane == 0) stage_ell(A, S, 0, jt, p_lo, p_hi);
+    for (int it = 0; it < ntiles; it++) {
+        const int j = jt - it;
+        const int slot = it & 1;
+        const int row0 = 32 * j;
+        const int a0 = max(lo, row0), a1 = min(hi, row0 + 32);
+        // stage tile j-1, prefetch its right-hand side and the pointer of tile j-2
+        int p_next2 = 0;
+        double rhs_n = 0.0;
+        if (it + 1 < ntiles) {
+            if (lane == 0) stage_ell(A, S, slot ^ 1, j - 1, p_next, p_lo);
+            rhs_n = load_rhs(j - 1);
+            if (it + 2 < ntiles) p_next2 = A.ell_ptr[j - 2];
+        }
+        {
+            const long long t0 = clock64();
+            while (!mbar_try_wait(&S.bar[slot], (phase >> slot) & 1u)) {
+                if (clock64() - t0 > kWaitCycles) {
+                    if (lane == 0) atomicExch(A.err, 1);
+                    return false;
+                }
+            }
+            phase ^= 1u << slot;
+        }
+        const int width = (p_hi - p_lo) >> 5;
+        const bool staged = width <= kEllCap;
+        const double *vb = staged ? S.v[slot] : A.ell_val + p_lo;
+        const int *cb = staged ? S.c[slot] : A.ell_col + p_lo;
+        const double *rdt = S.rd[slot];
+        const int row = row0 + lane;
+        const bool act = row >= a0 && row < a1;
+        const double rd = rdt[lane];
+        double acc = act ? rhs_c : 0.0;
+        double pacc[4] = {0.0, 0.0, 0.0, 0.0};
+        unsigned mask = 0u;
+        if (act) {
+            int k = 0;
+            for (; k + 4 <= width; k += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int c = cb[(k + u) * 32 + lane];
+                    const double v = vb[(k + u) * 32 + lane];
+                    if (c < a1) {
+                        S.coef[c - row0][lane] = v * rdt[c - row0];
+                        mask |= 1u << (c - row0);
+                    } else {
+                        pacc[u] = fma(v, tile_solved_x<FULL>(A, S, c, a1, hi_ext), pacc[u]);
+                    }
+                }
+            }
+            for (; k < width; k++) {
+                const int c = cb[k * 32 + lane];
+                const double v = vb[k * 32 + lane];
+                if (c < a1) {
+                    S.coef[c - row0][lane] = v * rdt[c - row0];
+                    mask |= 1u << (c - row0);
+                } else {
+                    pacc[0] = fma(v, tile_solved_x<FULL>(A, S, c, a1, hi_ext), pacc[0]);
+                }
+            }
+        }
+        acc -= (pacc[0] + pacc[1]) + (pacc[2] + pacc[3]);
+        __syncwarp();
+        // in-tile triangle over the active rows (bottom-up); a lane's accumulator
+        // is final after its own step
+        const int i_hi = a1 - 1 - row0, i_lo = a0 - row0;
+        if (i_hi == 31 && i_lo == 0) {
+#pragma unroll
+            for (int i = 31; i >= 0; i--) {
+                const double ci = S.coef[i][lane];
+                const double ai = __shfl_sync(FULLMASK, acc, i);
+                acc = fma(-ci, ai, acc);
+            }
+        } else {
+            for (int i = i_hi; i >= i_lo; i--) {
+                const double ci = S.coef[i][lane];
+                const double ai = __shfl_sync(FULLMASK, acc, i);
+                acc = fma(-ci, ai, acc);
+            }
+        }
+        const double myx = acc * rd;
+        while (mask) {
+            const int i = __ffs(mask) - 1;
+            S.coef[i][lane] = 0.0;
+            mask &= mask - 1u;
+        }
+        if (act) {
+            A.xout[A.rev_out ? n - 1 - row : row] = myx;
+            S.win[row & (kWin - 1)] = myx;
+        }
+        __syncwarp();
+        p_hi = p_lo;
+        p_lo = p_next;
+        p_next = p_next2;
+        rhs_c = rhs_n;
+    }
+    return true;
+}
+
+__device__ void tile_copy_rows(const SegArgs &A, TileSmem &S, int lo, int hi) {
+    const int lane = threadIdx.x & 31;
+    for (int r = lo + lane; r < hi; r += 32) {
+        const double v = A.xfix[r];
+        A.xout[A.rev_out ? A.n - 1 - r : r] = v;
+        if (r < lo + kWin) S.win[r & (kWin - 1)] = v;
+    }
+    __syncwarp();
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
+    __shared__ TileSmem S;
+    const int task = blockIdx.x;
+    if (task >= A.ntasks) return;
+    const int lane = threadIdx.x;
+    if (lane == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        fence_mbar_init();
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
+    __syncwarp();
+    unsigned phase = 0u;
+    const SegTask t = A.tasks[task];
+    if (FULL && t.tail > t.hi) tile_copy_rows(A, S, t.hi, t.tail);
+    if (t.skip_hi > t.skip_lo) {
+        if (!tile_range<FULL>(A, S, phase, t.skip_hi, t.hi, t.hi)) return;
+        tile_copy_rows(A, S, t.skip_lo, t.skip_hi);
+        tile_range<FULL>(A, S, phase, t.lo, t.skip_lo, t.hi);
+    } else {
+        tile_range<FULL>(A, S, phase, t.lo, t.hi, t.hi);
+    }
+}
+
+// sliced-ELL construction: widths per tile, then slots (padding: value 0, column = row)
+__global__ void k_ell_width(int n, const int *__restrict__ ia, int *__restrict__ width) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
+    int w = len;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if ((threadIdx.x & 31) == 0 && (r >> 5) < (n + 31) / 32) width[r >> 5] = w * 32;
+}
+
+__global__ void k_ell_fill(int n, int ntiles, const int *__restrict__ ia, const int *__restrict__ ja,
+                           const double *__restrict__ a, const int *__restrict__ ptr, double *__restrict__ ev,
+                           int *__restrict__ ec) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = r >> 5, l = r & 31;
+    if (j >= ntiles) return;
+    const int width = (ptr[j + 1] - ptr[j]) >> 5;
+    const int b = r < n ? ia[r] + 1 : 0, len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
+    const int self = r < n ? r : n - 1;
+    for (int k = 0; k < width; k++) {
+        const long long o = (long long)ptr[j] + 32 * k + l;
+        if (k < len) {
+            ev[o] = a[b + k];
+            ec[o] = ja[b + k];
+        } else {
+            ev[o] = 0.0;
+            ec[o] = self;
+        }
+    }
+}
+
+__global__ void k_reciprocal_diag(int n, const int *__restrict__ ia, const double *__restrict__ a,
+                                  double *__restrict__ rdiag) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) rdiag[r] = 1.0 / a[ia[r]];
 }
 
 __global__ void k_reverse(int n, const double *__restrict__ src, double *__restrict__ dst) {
@@ -482,6 +765,48 @@ int solve_prepare(spk_system *s) {
 
     SPK_TRY(s->xbuf.alloc(s->n));
     if (s->uplo == 'L') SPK_TRY(s->xout_u.alloc(s->n));
+    // 1 / diagonal of U, padded to whole 32-row tiles (staged 256 bytes per tile)
+    const int ntiles = (s->n + 31) / 32;
+    SPK_TRY(s->rdiag.alloc(32ll * ntiles + 32));
+    SPK_CUDA(cudaMemset(s->rdiag.p, 0, sizeof(double) * (32ll * ntiles + 32)));
+    k_reciprocal_diag<<<blocks_for(s->n), 256, 0, s->stream>>>(s->n, s->uia.p, s->ua.p, s->rdiag.p);
+    SPK_CUDA(cudaGetLastError());
+    // sliced ELL of the off-diagonals; kept when padding stays within 2x the off-diagonals
+    {
+        DBuf<int> width;
+        SPK_TRY(width.alloc(ntiles + 1));
+        SPK_CUDA(cudaMemsetAsync(width.p, 0, sizeof(int) * (ntiles + 1), s->stream));
+        k_ell_width<<<blocks_for(32ll * ntiles), 256, 0, s->stream>>>(s->n, s->uia.p, width.p);
+        SPK_CUDA(cudaGetLastError());
+        std::vector<int> hw(ntiles + 1);
+        SPK_CUDA(cudaStreamSynchronize(s->stream));
+        SPK_CUDA(cudaMemcpy(hw.data(), width.p, sizeof(int) * ntiles, cudaMemcpyDeviceToHost));
+        std::vector<int> ptr(ntiles + 1, 0);
+        long long tot = 0;
+        for (int j = 0; j < ntiles; j++) {
+            ptr[j] = (int)std::min<long long>(tot, 2147483647ll);
+            tot += hw[j];
+        }
+        const long long offdiag = (long long)s->nnz - s->n;
+        const char *no_ell = getenv("SPK_DISABLE_ELL");  // test hook: force the CSR segment solver
+        s->ell_ok = tot < 2147483647ll && tot <= 2 * std::max<long long>(offdiag, 1) + 32ll * ntiles &&
+                    !(no_ell && no_ell[0] == '1');
+        if (s->ell_ok) {
+            ptr[ntiles] = (int)tot;
+            SPK_TRY(upload(s->ell_ptr, ptr));
+            SPK_TRY(s->ell_val.alloc(std::max<long long>(tot, 1)));
+            SPK_TRY(s->ell_col.alloc(std::max<long long>(tot, 1)));
+            k_ell_fill<<<blocks_for(32ll * ntiles), 256, 0, s->stream>>>(s->n, ntiles, s->uia.p, s->uja.p, s->ua.p,
+                                                                         s->ell_ptr.p, s->ell_val.p, s->ell_col.p);
+            SPK_CUDA(cudaGetLastError());
+        } else {
+            s->ell_val.release();
+            s->ell_col.release();
+            s->ell_ptr.release();
+        }
+        s->ell_entries = s->ell_ok ? tot : 0;
+    }
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
     SPK_TRY(s->d_err.alloc(1));
     SPK_CUDA(cudaMemset(s->d_err.p, 0, sizeof(int)));
     return SPK_OK;
@@ -512,6 +837,10 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
     A.ia = s->uia.p;
     A.ja = s->uja.p;
     A.a = s->ua.p;
+    A.rdiag = s->rdiag.p;
+    A.ell_val = s->ell_val.p;
+    A.ell_col = s->ell_col.p;
+    A.ell_ptr = s->ell_ptr.p;
     A.n = s->n;
     A.rhs = b;
     A.rev_in = s->uplo == 'L';
@@ -522,7 +851,8 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         A.xfix = nullptr;
         A.xout = s->xbuf.p;
         A.rev_out = 0;
-        k_segment_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
+        if (s->ell_ok) k_tile_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
+        else k_segment_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
         SPK_CUDA(cudaGetLastError());
         s->launches++;
     }
@@ -541,7 +871,8 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
     A.xfix = s->xbuf.p;
     A.xout = x;
     A.rev_out = s->uplo == 'L';
-    k_segment_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
+    if (s->ell_ok) k_tile_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
+    else k_segment_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
     SPK_CUDA(cudaGetLastError());
     s->launches++;
     if (prof) {

@@ -130,7 +130,11 @@ struct spk_system {
     spk::DBuf<spk::SegTask> d_tasks1, d_tasks2;
     int ntasks1 = 0, ntasks2 = 0;
     long long rows_phase1 = 0, rows_phase4 = 0;  // rows solved per call by phase 1 / phase 4
-    spk::DBuf<double> xbuf, xout_u;
+    spk::DBuf<double> xbuf, xout_u, rdiag;
+    spk::DBuf<double> ell_val;  // sliced ELL of U's off-diagonals (32-row tiles)
+    spk::DBuf<int> ell_col, ell_ptr;
+    int ell_ok = 0;
+    long long ell_entries = 0;
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     // optional per-phase device timing (spk_set_profiling)

@@ -236,3 +236,26 @@ def test_truncation_engages_on_decaying_spikes_and_stays_accurate():
     xe = E.solve(b)
     assert rel_err(xe, xs) <= TOL
     assert rel_err(x, xe) <= 1e-15
+
+
+def test_csr_fallback_solver_matches_oracle(monkeypatch):
+    """The CSR segment solver (used when the sliced-ELL layout would pad too much)."""
+    monkeypatch.setenv("SPK_DISABLE_ELL", "1")
+    for name, A, P in random_cases(12):
+        O = oracle.Oracle()
+        O.preproc(A, P, uplo="U", flb=1)
+        S = gpu_system(A, P, "U", 1)
+        assert S.scalar("ell") == 0
+        _, b = synth.make_rhs(A, seed=1)
+        assert rel_err(S.solve(b), O.solve(b)) <= TOL, name
+    L = synth.banded_lower(100000, seed=3)
+    x_true, b = synth.make_rhs(L, seed=3)
+    S = gpu_system(L, 64, "L", 1)
+    assert rel_err(S.solve(b), x_true) <= TOL
+
+
+def test_ell_layout_is_used_for_banded():
+    L = synth.banded_lower(10000, seed=3)
+    S = gpu_system(L, 8, "L", 1)
+    assert S.scalar("ell") == 1
+    assert S.scalar("ell_entries") == 16 * 32 * ((L.m + 31) // 32)
