@@ -258,4 +258,7 @@ def test_ell_layout_is_used_for_banded():
     L = synth.banded_lower(10000, seed=3)
     S = gpu_system(L, 8, "L", 1)
     assert S.scalar("ell") == 1
-    assert S.scalar("ell_entries") == 16 * 32 * ((L.m + 31) // 32)
+    U = synth.mirror(L)
+    offd = np.diff(U.ia) - 1
+    widths = [int(offd[j:j + 32].max()) for j in range(0, U.m, 32)]
+    assert S.scalar("ell_entries") == 32 * sum(widths)
