@@ -372,7 +372,7 @@ struct TileSmem {
     alignas(128) double v[2][kEllCap * 32];
     alignas(128) int c[2][kEllCap * 32];
     alignas(128) double rd[2][32];     // 1 / diagonal of the tile's rows
-    alignas(16) double coef[32][32];   // [tile column i][lane row l] = a(l, i) / a(i, i)
+    alignas(16) double coef[33][32];   // [tile column i][lane row l] = a(l, i) / a(i, i); row 32: scratch
     double win[kWin];                  // x of the last kWin solved rows, by row mod kWin
     alignas(8) unsigned long long bar[2];
 };
@@ -380,12 +380,11 @@ struct TileSmem {
 // Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and, when it
 // is at most kEllCap slots wide, its values and columns.
 __device__ __forceinline__ void stage_ell(const SegArgs &A, TileSmem &S, int slot, int j, int e0, int e1) {
-    const unsigned ne = (unsigned)(e1 - e0);
-    const bool staged = ne <= (unsigned)(kEllCap * 32);
+    const unsigned ne = (unsigned)min(e1 - e0, kEllCap * 32);  // the first kEllCap slots
     fence_proxy_async();
-    mbar_arrive_expect_tx(&S.bar[slot], 256u + (staged ? ne * 12u : 0u));
+    mbar_arrive_expect_tx(&S.bar[slot], 256u + ne * 12u);
     bulk_g2s(S.rd[slot], A.rdiag + 32ll * j, 256u, &S.bar[slot]);
-    if (staged && ne) {
+    if (ne) {
         bulk_g2s(S.v[slot], A.ell_val + e0, ne * 8u, &S.bar[slot]);
         bulk_g2s(S.c[slot], A.ell_col + e0, ne * 4u, &S.bar[slot]);
     }
@@ -440,39 +439,50 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
             phase ^= 1u << slot;
         }
         const int width = (p_hi - p_lo) >> 5;
-        const bool staged = width <= kEllCap;
-        const double *vb = staged ? S.v[slot] : A.ell_val + p_lo;
-        const int *cb = staged ? S.c[slot] : A.ell_col + p_lo;
+        const int nst = min(width, kEllCap);  // staged slots; the rest are read from global memory
         const double *rdt = S.rd[slot];
         const int row = row0 + lane;
         const bool act = row >= a0 && row < a1;
         const double rd = rdt[lane];
         double acc = act ? rhs_c : 0.0;
         double pacc[4] = {0.0, 0.0, 0.0, 0.0};
-        unsigned mask = 0u;
+        bool slow = false;
+        // Branch-free slot step: in-tile columns store a(r, c) / a(c, c) into the
+        // coefficient tile (others into the scratch row), columns inside the
+        // shared window are summed; columns beyond the window or past hi_ext are
+        // flagged for the slow pass below.
+        auto slot_step = [&](int c, double v, double &pa) {
+            const bool in_tile = c < a1;
+            const int ci = in_tile ? c - row0 : 32;
+            S.coef[ci][lane] = v * rdt[ci & 31];
+            const double w = S.win[c & (kWin - 1)];
+            const bool in_win = !in_tile && c < hi_ext && c < a1 + kWin;
+            pa = in_win ? fma(v, w, pa) : pa;
+            slow = slow || (!in_tile && !in_win && (FULL || c < hi_ext));
+        };
         if (act) {
+            const double *vs = S.v[slot];
+            const int *cs = S.c[slot];
             int k = 0;
-            for (; k + 4 <= width; k += 4) {
+            for (; k + 4 <= nst; k += 4) {
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int c = cb[(k + u) * 32 + lane];
-                    const double v = vb[(k + u) * 32 + lane];
-                    if (c < a1) {
-                        S.coef[c - row0][lane] = v * rdt[c - row0];
-                        mask |= 1u << (c - row0);
-                    } else {
-                        pacc[u] = fma(v, tile_solved_x<FULL>(A, S, c, a1, hi_ext), pacc[u]);
-                    }
-                }
+                for (int u = 0; u < 4; u++) slot_step(cs[(k + u) * 32 + lane], vs[(k + u) * 32 + lane], pacc[u]);
             }
-            for (; k < width; k++) {
-                const int c = cb[k * 32 + lane];
-                const double v = vb[k * 32 + lane];
-                if (c < a1) {
-                    S.coef[c - row0][lane] = v * rdt[c - row0];
-                    mask |= 1u << (c - row0);
-                } else {
-                    pacc[0] = fma(v, tile_solved_x<FULL>(A, S, c, a1, hi_ext), pacc[0]);
+            for (; k < nst; k++) slot_step(cs[k * 32 + lane], vs[k * 32 + lane], pacc[0]);
+            const double *vg = A.ell_val + p_lo;
+            const int *cg = A.ell_col + p_lo;
+            for (; k < width; k++) slot_step(cg[k * 32 + lane], vg[k * 32 + lane], pacc[1]);
+        }
+        if (__any_sync(FULLMASK, slow) && act) {
+            // columns solved long ago (beyond the window) or fixed by phases 1-2
+            for (int k = 0; k < width; k++) {
+                const int c = k < nst ? S.c[slot][k * 32 + lane] : A.ell_col[p_lo + k * 32 + lane];
+                const double v = k < nst ? S.v[slot][k * 32 + lane] : A.ell_val[p_lo + k * 32 + lane];
+                if (c < a1) continue;
+                if (c < hi_ext) {
+                    if (c >= a1 + kWin) pacc[2] = fma(v, A.xout[A.rev_out ? n - 1 - c : c], pacc[2]);
+                } else if (FULL) {
+                    pacc[3] = fma(v, A.xfix[c], pacc[3]);
                 }
             }
         }
@@ -496,11 +506,9 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
             }
         }
         const double myx = acc * rd;
-        while (mask) {
-            const int i = __ffs(mask) - 1;
-            S.coef[i][lane] = 0.0;
-            mask &= mask - 1u;
-        }
+        // leave the coefficient tile zero for the next tile
+#pragma unroll
+        for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
         if (act) {
             A.xout[A.rev_out ? n - 1 - row : row] = myx;
             S.win[row & (kWin - 1)] = myx;
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
         fence_mbar_init();
     }
 #pragma unroll
-    for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
+    for (int i = 0; i < 33; i++) S.coef[i][lane] = 0.0;
     __syncwarp();
     unsigned phase = 0u;
     const SegTask t = A.tasks[task];
