@@ -451,27 +451,50 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         // coefficient tile (others into the scratch row), columns inside the
         // shared window are summed; columns beyond the window or past hi_ext are
         // flagged for the slow pass below.
-        auto slot_step = [&](int c, double v, double &pa) {
-            const bool in_tile = c < a1;
-            const int ci = in_tile ? c - row0 : 32;
-            S.coef[ci][lane] = v * rdt[ci & 31];
-            const double w = S.win[c & (kWin - 1)];
-            const bool in_win = !in_tile && c < hi_ext && c < a1 + kWin;
-            pa = in_win ? fma(v, w, pa) : pa;
-            slow = slow || (!in_tile && !in_win && (FULL || c < hi_ext));
-        };
+        // Slots in chunks of 8: all loads of a chunk are issued before its shared
+        // stores (the stores may alias the staged buffers, so loads cannot move
+        // past them).  In-tile columns store a(r, c) / a(c, c) into the
+        // coefficient tile (others into the scratch row); columns inside the
+        // shared window are summed; columns beyond the window or past hi_ext are
+        // flagged for the slow pass.
         if (act) {
             const double *vs = S.v[slot];
             const int *cs = S.c[slot];
-            int k = 0;
-            for (; k + 4 <= nst; k += 4) {
-#pragma unroll
-                for (int u = 0; u < 4; u++) slot_step(cs[(k + u) * 32 + lane], vs[(k + u) * 32 + lane], pacc[u]);
-            }
-            for (; k < nst; k++) slot_step(cs[k * 32 + lane], vs[k * 32 + lane], pacc[0]);
             const double *vg = A.ell_val + p_lo;
             const int *cg = A.ell_col + p_lo;
-            for (; k < width; k++) slot_step(cg[k * 32 + lane], vg[k * 32 + lane], pacc[1]);
+            for (int k0 = 0; k0 < width; k0 += 8) {
+                int cr[8];
+                double vr[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int k = k0 + u;
+                    if (k < nst) {
+                        cr[u] = cs[k * 32 + lane];
+                        vr[u] = vs[k * 32 + lane];
+                    } else if (k < width) {
+                        cr[u] = cg[k * 32 + lane];
+                        vr[u] = vg[k * 32 + lane];
+                    } else {
+                        cr[u] = row;  // no-op slot: zero into the row's own (diagonal) position
+                        vr[u] = 0.0;
+                    }
+                }
+                int ci[8];
+                double rr[8], wr[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    ci[u] = cr[u] < a1 ? cr[u] - row0 : 32;
+                    rr[u] = rdt[ci[u] & 31];
+                    wr[u] = S.win[cr[u] & (kWin - 1)];
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    S.coef[ci[u]][lane] = vr[u] * rr[u];
+                    const bool in_win = ci[u] == 32 && cr[u] < hi_ext && cr[u] < a1 + kWin;
+                    pacc[u & 3] = in_win ? fma(vr[u], wr[u], pacc[u & 3]) : pacc[u & 3];
+                    slow = slow || (ci[u] == 32 && !in_win && (FULL || cr[u] < hi_ext));
+                }
+            }
         }
         if (__any_sync(FULLMASK, slow) && act) {
             // columns solved long ago (beyond the window) or fixed by phases 1-2
@@ -524,10 +547,21 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
 
 __device__ void tile_copy_rows(const SegArgs &A, TileSmem &S, int lo, int hi) {
     const int lane = threadIdx.x & 31;
-    for (int r = lo + lane; r < hi; r += 32) {
-        const double v = A.xfix[r];
-        A.xout[A.rev_out ? A.n - 1 - r : r] = v;
-        if (r < lo + kWin) S.win[r & (kWin - 1)] = v;
+    for (int r0 = lo; r0 < hi; r0 += 32 * 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int r = r0 + 32 * u + lane;
+            v[u] = r < hi ? A.xfix[r] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int r = r0 + 32 * u + lane;
+            if (r < hi) {
+                A.xout[A.rev_out ? A.n - 1 - r : r] = v[u];
+                if (r < lo + kWin) S.win[r & (kWin - 1)] = v[u];
+            }
+        }
     }
     __syncwarp();
 }
@@ -556,6 +590,46 @@ __global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
     } else {
         tile_range<FULL>(A, S, phase, t.lo, t.hi, t.hi);
     }
+}
+
+// ---- internal spikes for coupled blocks the reference gives no spike --------------
+//
+// For rows [ps, rl] of a block (rl = its last coupling row), x - y = -W x_c with
+// W = D^{-1} R over the block's rows [ps, rl] (D: entries at columns <= rl; R:
+// entries at the coupling columns >= pe, compressed to the distinct ones).  Rows
+// whose W row sums to <= tau keep the block-local value in phase 4.  One thread
+// per coupling column sweeps the rows bottom-up; W lives in a scratch matrix.
+
+__global__ void k_aux_sweep(int ps, int rl, int pe, const int *__restrict__ ia, const int *__restrict__ ja,
+                            const double *__restrict__ a, const int *__restrict__ cols, int ncols,
+                            double *__restrict__ W) {
+    for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
+        const int cj = cols[j];
+        for (int r = rl; r >= ps; r--) {
+            const int b = ia[r], e = ia[r + 1];
+            // coupling entry (r, cj), if any: binary search in the row's sorted columns
+            int lo = b, hi = e;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (ja[mid] < cj) lo = mid + 1; else hi = mid;
+            }
+            double acc = (lo < e && ja[lo] == cj) ? a[lo] : 0.0;
+            for (int q = b + 1; q < e; q++) {
+                const int c = ja[q];
+                if (c > rl) break;
+                acc -= a[q] * W[(long long)(c - ps) * ncols + j];
+            }
+            W[(long long)(r - ps) * ncols + j] = acc / a[b];
+        }
+    }
+}
+
+__global__ void k_aux_first(int rows, int ncols, const double *__restrict__ W, double tau, int *__restrict__ first) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    double s = 0.0;
+    for (int j = 0; j < ncols; j++) s += fabs(W[(long long)r * ncols + j]);
+    if (s > tau) atomicMin(first, r);
 }
 
 // sliced-ELL construction: widths per tile, then slots (padding: value 0, column = row)
@@ -706,10 +780,62 @@ int solve_prepare(spk_system *s) {
             for (int t = 0; t < P; t++) first[t] = 0;
         }
     }
+    // internal spikes: coupled blocks whose phase-4 range would not be truncated
+    std::vector<int> aux_first(P, -1);  // >= 0: rows [ps, ps+aux_first) keep y
+    if (tau >= 0 && s->redNec) {
+        std::vector<int> hia(s->n + 1);
+        bool have_ia = false;
+        for (int t = 0; t < P; t++) {
+            const Part &p = s->parts[t];
+            const bool split = p.hasRefl || p.isOpt;
+            const bool banded_trunc = split && p.hasS && p.nRowsS > 0;
+            const int rl = p.maxIR;  // last row with a coupling column
+            if (banded_trunc || rl < p.ps || rl + 1 - p.ps < 256 || p.pe >= s->n) continue;
+            if (!have_ia) {
+                SPK_CUDA(cudaMemcpy(hia.data(), s->uia.p, sizeof(int) * (s->n + 1), cudaMemcpyDeviceToHost));
+                have_ia = true;
+            }
+            // distinct coupling columns of rows [ps, rl]
+            const int e0 = hia[p.ps], e1 = hia[rl + 1];
+            std::vector<int> hja(e1 - e0);
+            SPK_CUDA(cudaMemcpy(hja.data(), s->uja.p + e0, sizeof(int) * (e1 - e0), cudaMemcpyDeviceToHost));
+            std::vector<int> cols;
+            for (int c : hja)
+                if (c >= p.pe) cols.push_back(c);
+            std::sort(cols.begin(), cols.end());
+            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+            if (cols.empty() || cols.size() > 1024) continue;
+            const int rows = rl + 1 - p.ps, nc = (int)cols.size();
+            DBuf<int> d_cols, d_first;
+            DBuf<double> W;
+            SPK_TRY(upload(d_cols, cols));
+            SPK_TRY(W.alloc((size_t)rows * nc));
+            SPK_TRY(d_first.alloc(1));
+            SPK_CUDA(cudaMemcpy(d_first.p, &rows, sizeof(int), cudaMemcpyHostToDevice));
+            k_aux_sweep<<<1, ((nc + 31) / 32) * 32, 0, s->stream>>>(p.ps, rl, p.pe, s->uia.p, s->uja.p, s->ua.p,
+                                                                    d_cols.p, nc, W.p);
+            k_aux_first<<<blocks_for(rows), 256, 0, s->stream>>>(rows, nc, W.p, tau, d_first.p);
+            SPK_CUDA(cudaGetLastError());
+            int f = rows;
+            SPK_CUDA(cudaMemcpy(&f, d_first.p, sizeof(int), cudaMemcpyDeviceToHost));
+            aux_first[t] = f;
+        }
+    }
     std::vector<SegTask> t1, t2;
     long long rows1 = 0, rows2 = 0;
     for (int t = 0; t < P; t++) {
         const Part &p = s->parts[t];
+        if (aux_first[t] >= 0) {
+            // block-local y over the whole block in phase 1; phase 4 recomputes rows
+            // [ps + aux_first, last coupling row] and keeps y elsewhere
+            t1.push_back(SegTask{p.ps, p.pe, 0, 0, p.pe});
+            rows1 += p.pe - p.ps;
+            const int hi = p.maxIR + 1;
+            SegTask k{p.ps, hi, p.ps, p.ps + std::min(aux_first[t], hi - p.ps), p.pe};
+            rows2 += (hi - p.ps) - (k.skip_hi - k.skip_lo);
+            t2.push_back(k);
+            continue;
+        }
         const bool split = s->redNec && (p.hasRefl || p.isOpt);
         if (split) {
             // D1 rows [ps+si, pe); a cut before the block (si < 0) adds a row of the
