@@ -816,6 +816,7 @@ int solve_prepare(spk_system *s) {
                                                                     d_cols.p, nc, W.p);
             k_aux_first<<<blocks_for(rows), 256, 0, s->stream>>>(rows, nc, W.p, tau, d_first.p);
             SPK_CUDA(cudaGetLastError());
+            SPK_CUDA(cudaStreamSynchronize(s->stream));  // the stream does not sync with cudaMemcpy
             int f = rows;
             SPK_CUDA(cudaMemcpy(&f, d_first.p, sizeof(int), cudaMemcpyDeviceToHost));
             aux_first[t] = f;
