@@ -281,12 +281,13 @@ def run_ours(args):
     peak, peak_kind = peaks()
     achieved = seg_bytes / (seg_ms * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "segment_solve_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "tile_solve_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tr = json.load(f)
-        if "dram_bytes_per_row" in tr:
-            traffic = tr["dram_bytes_per_row"] * (rows1 + rows4) / 2  # per launch (2 launches per solve)
+        # DRAM bytes per launch of the segment-solver kernel, scaled from the ncu
+        # capture of the same kernel by rows solved (traffic grows with the rows)
+        traffic = (tr["phase1_dram_bytes_per_row"] * rows1 + tr["phase4_dram_bytes_per_row"] * rows4) / 2 / 1e9
 
     # end to end through the reference-facing C ABI with pinned host buffers
     bh = torch.from_numpy(b).pin_memory()
@@ -328,7 +329,8 @@ def run_ours(args):
                           "per_gpu": "each rank solves its own copy (weak scaling)"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                            "kernel": "k_segment_solve (phase 1 D1 sweep + phase 3/4 coupled D2 sweep)",
+                            "kernel": "k_tile_solve (phase 1 D1 sweep + phase 3/4 coupled D2 sweep), 2 launches per solve",
+                            "traffic_unit": "GB per launch (ncu DRAM bytes per row x rows, averaged over the 2 launches)",
                             "algorithmic_bytes_per_solve": B,
                             "whole_solve_gbs": B / (ms_max * 1e-3) / 1e9},
                "phases_ms": {"d1_local": ph[0], "reduced": ph[1], "d2_coupled": ph[2],

@@ -51,3 +51,26 @@ def test_reference_flag_defaults():
 def test_no_cpu_fallback_without_gpu():
     with pytest.raises(capi.SpkError):
         capi.System()
+
+
+def build_c_driver(tmp_path):
+    exe = str(tmp_path / "example_driver")
+    src = os.path.join(ROOT, "tests", "c", "example_driver.c")
+    libdir = os.path.dirname(build.LIB)
+    subprocess.run(["/usr/bin/gcc", "-O2", "-o", exe, src, "-I" + os.path.join(ROOT, "include"),
+                    "-L" + libdir, "-lspike_pstrsv_b200", "-Wl,-rpath," + libdir, "-lm"], check=True)
+    return exe
+
+
+def test_c_caller_compiles_and_links(tmp_path):
+    """A C program in the reference's example_usage.c call pattern builds against
+    include/spike_pstrsv.h and links libspike_pstrsv_b200.so."""
+    assert os.path.exists(build_c_driver(tmp_path))
+
+
+@pytest.mark.gpu
+def test_c_caller_runs(tmp_path):
+    exe = build_c_driver(tmp_path)
+    out = subprocess.run([exe, "96", "6"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "Reduced system size" in out.stdout  # logPSTRSV3 text format
