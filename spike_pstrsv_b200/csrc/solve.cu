@@ -372,7 +372,8 @@ struct TileSmem {
     alignas(128) double v[2][kEllCap * 32];
     alignas(128) int c[2][kEllCap * 32];
     alignas(128) double rd[2][32];     // 1 / diagonal of the tile's rows
-    alignas(16) double coef[32][32];   // [tile column i][lane row l] = a(l, i) / a(i, i), valid where the lane's mask bit i is set
+    alignas(16) double coef[33][32];   // [tile column i][lane row l] = a(l, i) / a(i, i), valid where the
+                                       // lane's mask bit i is set; row 32 takes the no-op stores
     double win[kWin];                  // x of the last kWin solved rows, by row mod kWin
     alignas(8) unsigned long long bar[2];
 };
@@ -453,9 +454,10 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         // stores (the stores may alias the staged buffers, so loads cannot move
         // past them).  In-tile columns store a(r, c) / a(c, c) into the
         // coefficient tile and set the lane's mask bit (the chain selects by mask,
-        // so the tile never needs clearing); columns inside the shared window are
-        // summed; columns beyond the window or past hi_ext are flagged for the
-        // slow pass.  Loads and stores are predicated to the lanes that use them.
+        // so the tile never needs clearing; other slots store into row 32); columns
+        // inside the shared window are summed; columns beyond the window or past
+        // hi_ext are flagged for the slow pass.  No branches: every lane issues the
+        // same loads and stores.
         if (act) {
             const double *vs = S.v[slot];
             const int *cs = S.c[slot];
@@ -482,21 +484,18 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
                 double rr[8], wr[8];
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
-                    ci[u] = cr[u] - row0;
-                    const bool in_tile = cr[u] < a1;
-                    rr[u] = in_tile ? rdt[ci[u]] : 0.0;
-                    wr[u] = in_tile ? 0.0 : S.win[cr[u] & (kWin - 1)];
+                    const bool in_tile = cr[u] < a1 && cr[u] != row;
+                    ci[u] = in_tile ? cr[u] - row0 : 32;
+                    rr[u] = rdt[ci[u] & 31];
+                    wr[u] = S.win[cr[u] & (kWin - 1)];
                 }
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
-                    const bool in_tile = cr[u] < a1;
-                    if (in_tile && ci[u] != lane) {
-                        S.coef[ci[u]][lane] = vr[u] * rr[u];
-                        mask |= 1u << ci[u];
-                    }
-                    const bool in_win = !in_tile && cr[u] < hi_ext && cr[u] < a1 + kWin;
+                    S.coef[ci[u]][lane] = vr[u] * rr[u];
+                    mask |= ci[u] < 32 ? 1u << (ci[u] & 31) : 0u;
+                    const bool in_win = cr[u] >= a1 && cr[u] < hi_ext && cr[u] < a1 + kWin;
                     pacc[u & 3] = in_win ? fma(vr[u], wr[u], pacc[u & 3]) : pacc[u & 3];
-                    slow = slow || (!in_tile && !in_win && (FULL || cr[u] < hi_ext));
+                    slow = slow || (cr[u] >= a1 && !in_win && (FULL || cr[u] < hi_ext));
                 }
             }
         }
@@ -521,13 +520,15 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         if (i_hi == 31 && i_lo == 0) {
 #pragma unroll
             for (int i = 31; i >= 0; i--) {
-                const double ci = (mask >> i) & 1u ? S.coef[i][lane] : 0.0;
+                const double cv = S.coef[i][lane];
+                const double ci = (mask >> i) & 1u ? cv : 0.0;
                 const double ai = __shfl_sync(FULLMASK, acc, i);
                 acc = fma(-ci, ai, acc);
             }
         } else {
             for (int i = i_hi; i >= i_lo; i--) {
-                const double ci = (mask >> i) & 1u ? S.coef[i][lane] : 0.0;
+                const double cv = S.coef[i][lane];
+                const double ci = (mask >> i) & 1u ? cv : 0.0;
                 const double ai = __shfl_sync(FULLMASK, acc, i);
                 acc = fma(-ci, ai, acc);
             }
