@@ -372,8 +372,7 @@ struct TileSmem {
     alignas(128) double v[2][kEllCap * 32];
     alignas(128) int c[2][kEllCap * 32];
     alignas(128) double rd[2][32];     // 1 / diagonal of the tile's rows
-    alignas(16) double coef[33][32];   // [tile column i][lane row l] = a(l, i) / a(i, i), valid where the
-                                       // lane's mask bit i is set; row 32 takes the no-op stores
+    alignas(16) double coef[33][32];   // [tile column i][lane row l] = a(l, i) / a(i, i); row 32: scratch
     double win[kWin];                  // x of the last kWin solved rows, by row mod kWin
     alignas(8) unsigned long long bar[2];
 };
@@ -381,9 +380,8 @@ struct TileSmem {
 // Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and, when it
 // is at most kEllCap slots wide, its values and columns.
 __device__ __forceinline__ void stage_ell(const SegArgs &A, TileSmem &S, int slot, int j, int e0, int e1) {
-    // No proxy fence: the slot's previous contents were only read by generic loads
-    // whose values were consumed before this issue (a read-then-overwrite reuse).
     const unsigned ne = (unsigned)min(e1 - e0, kEllCap * 32);  // the first kEllCap slots
+    fence_proxy_async();
     mbar_arrive_expect_tx(&S.bar[slot], 256u + ne * 12u);
     bulk_g2s(S.rd[slot], A.rdiag + 32ll * j, 256u, &S.bar[slot]);
     if (ne) {
@@ -449,15 +447,16 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         double acc = act ? rhs_c : 0.0;
         double pacc[4] = {0.0, 0.0, 0.0, 0.0};
         bool slow = false;
-        unsigned mask = 0u;  // in-tile columns holding a coefficient of this lane's row
+        // Branch-free slot step: in-tile columns store a(r, c) / a(c, c) into the
+        // coefficient tile (others into the scratch row), columns inside the
+        // shared window are summed; columns beyond the window or past hi_ext are
+        // flagged for the slow pass below.
         // Slots in chunks of 8: all loads of a chunk are issued before its shared
         // stores (the stores may alias the staged buffers, so loads cannot move
         // past them).  In-tile columns store a(r, c) / a(c, c) into the
-        // coefficient tile and set the lane's mask bit (the chain selects by mask,
-        // so the tile never needs clearing; other slots store into row 32); columns
-        // inside the shared window are summed; columns beyond the window or past
-        // hi_ext are flagged for the slow pass.  No branches: every lane issues the
-        // same loads and stores.
+        // coefficient tile (others into the scratch row); columns inside the
+        // shared window are summed; columns beyond the window or past hi_ext are
+        // flagged for the slow pass.
         if (act) {
             const double *vs = S.v[slot];
             const int *cs = S.c[slot];
@@ -484,18 +483,16 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
                 double rr[8], wr[8];
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
-                    const bool in_tile = cr[u] < a1 && cr[u] != row;
-                    ci[u] = in_tile ? cr[u] - row0 : 32;
+                    ci[u] = cr[u] < a1 ? cr[u] - row0 : 32;
                     rr[u] = rdt[ci[u] & 31];
                     wr[u] = S.win[cr[u] & (kWin - 1)];
                 }
 #pragma unroll
                 for (int u = 0; u < 8; u++) {
                     S.coef[ci[u]][lane] = vr[u] * rr[u];
-                    mask |= ci[u] < 32 ? 1u << (ci[u] & 31) : 0u;
-                    const bool in_win = cr[u] >= a1 && cr[u] < hi_ext && cr[u] < a1 + kWin;
+                    const bool in_win = ci[u] == 32 && cr[u] < hi_ext && cr[u] < a1 + kWin;
                     pacc[u & 3] = in_win ? fma(vr[u], wr[u], pacc[u & 3]) : pacc[u & 3];
-                    slow = slow || (cr[u] >= a1 && !in_win && (FULL || cr[u] < hi_ext));
+                    slow = slow || (ci[u] == 32 && !in_win && (FULL || cr[u] < hi_ext));
                 }
             }
         }
@@ -520,20 +517,21 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         if (i_hi == 31 && i_lo == 0) {
 #pragma unroll
             for (int i = 31; i >= 0; i--) {
-                const double cv = S.coef[i][lane];
-                const double ci = (mask >> i) & 1u ? cv : 0.0;
+                const double ci = S.coef[i][lane];
                 const double ai = __shfl_sync(FULLMASK, acc, i);
                 acc = fma(-ci, ai, acc);
             }
         } else {
             for (int i = i_hi; i >= i_lo; i--) {
-                const double cv = S.coef[i][lane];
-                const double ci = (mask >> i) & 1u ? cv : 0.0;
+                const double ci = S.coef[i][lane];
                 const double ai = __shfl_sync(FULLMASK, acc, i);
                 acc = fma(-ci, ai, acc);
             }
         }
         const double myx = acc * rd;
+        // leave the coefficient tile zero for the next tile
+#pragma unroll
+        for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
         if (act) {
             A.xout[A.rev_out ? n - 1 - row : row] = myx;
             S.win[row & (kWin - 1)] = myx;
@@ -579,6 +577,8 @@ __global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
         mbar_init(&S.bar[1], 1);
         fence_mbar_init();
     }
+#pragma unroll
+    for (int i = 0; i < 33; i++) S.coef[i][lane] = 0.0;
     __syncwarp();
     unsigned phase = 0u;
     const SegTask t = A.tasks[task];
