@@ -144,6 +144,21 @@ int spk_solve_device(spk_system *s, const double *b, double *x, void *stream);
 /* Solve with host or device pointers; synchronous. */
 int spk_solve(spk_system *s, const double *b, double *x);
 
+/* Batched solve of nrhs right-hand sides, device arrays, column-major (column k
+ * of B at B + k*ldb, of X at X + k*ldx), asynchronous on `stream` unless a
+ * residual is requested or tol >= 0.  The matrix is read once per group of up
+ * to 16 right-hand sides.
+ *   mode SPK_MODE_FP64:    FP64 tile solves.
+ *   mode SPK_MODE_FP32_IR: FP32 tile solves (FP32 values, FP32 accumulation), FP64
+ *     residual R = B - A X and FP64 update X += solve_fp32(R), repeated until the
+ *     scaled residual ||R||inf / (||A||inf ||X||inf + ||B||inf) of every column is
+ *     <= tol (tol < 0: exactly maxit corrections, no host synchronisation).
+ * iters (optional) receives the corrections applied, resid (optional, forces a
+ * final residual) the largest scaled residual. */
+enum { SPK_MODE_FP64 = 0, SPK_MODE_FP32_IR = 1 };
+int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
+                    double tol, int maxit, void *stream, int *iters, double *resid);
+
 /* Wait for the system's work and report a device-side failure (a bounded wait
  * in a kernel that gave up) as SPK_ERR_TIMEOUT. */
 int spk_check(spk_system *s);

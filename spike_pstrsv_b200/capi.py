@@ -61,6 +61,8 @@ def lib() -> ctypes.CDLL:
         L.spk_set_truncation.argtypes = [vp, d]
         L.spk_check.argtypes = [vp]
         L.spk_set_profiling.argtypes = [vp, i]
+        L.spk_solve_batch.argtypes = [vp, i, vp, ctypes.c_longlong, vp, ctypes.c_longlong, i, d, i, vp,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
         L.spk_phase_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
     return _lib
@@ -231,6 +233,20 @@ class System:
         """Spike truncation threshold (default 2^-60); tau < 0 = exact mode."""
         _check(lib().spk_set_truncation(self.h, float(tau)))
         return self
+
+    def solve_batch(self, B, X, mode: int = 0, tol: float = 1e-12, maxit: int = 5, stream: int = 0,
+                    want_resid: bool = True):
+        """Batched solve of the columns of B (CUDA tensors, shape (nrhs, n): row k is
+        right-hand side k).  mode 0: FP64; mode 1: FP32 solves + FP64 refinement.
+        Returns (corrections applied, largest scaled residual or None)."""
+        nrhs, n = B.shape
+        it = ctypes.c_int(0)
+        r = ctypes.c_double(-1.0)
+        _check(lib().spk_solve_batch(self.h, int(nrhs), ctypes.c_void_p(B.data_ptr()), int(B.stride(0)),
+                                     ctypes.c_void_p(X.data_ptr()), int(X.stride(0)), int(mode), float(tol),
+                                     int(maxit), ctypes.c_void_p(stream), ctypes.byref(it),
+                                     ctypes.byref(r) if want_resid else None))
+        return it.value, (r.value if want_resid else None)
 
     def set_profiling(self, on: bool = True) -> "System":
         _check(lib().spk_set_profiling(self.h, int(on)))

@@ -375,6 +375,19 @@ int spk_check(spk_system *s) {
     return check_device_error(s);
 }
 
+int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
+                    double tol, int maxit, void *stream, int *iters, double *resid) {
+    if (!s || !B || !X) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!is_device_pointer(B) || !is_device_pointer(X)) {
+        set_error(SPK_ERR_ARG, "spk_solve_batch takes device arrays");
+        return SPK_ERR_ARG;
+    }
+    return solve_batch(s, nrhs, B, ldb, X, ldx, mode, tol, maxit, (cudaStream_t)stream, iters, resid);
+}
+
 int spk_set_profiling(spk_system *s, int on) {
     if (!s) {
         set_error(SPK_ERR_ARG, "null argument");
@@ -439,6 +452,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->JT.bytes() + s->mapR.bytes() + s->dep.bytes() + s->mapRedX.bytes() + s->xbuf.bytes();
         b += s->xout_u.bytes() + s->d_tasks1.bytes() + s->d_tasks2.bytes() + s->d_red_rows.bytes();
         b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
+        b += s->ell_valf.bytes() + s->rdiagf.bytes() + s->diag.bytes() + s->rbuf.bytes() + s->dbuf.bytes() + s->work.bytes();
         return b;
     }
     return -1;

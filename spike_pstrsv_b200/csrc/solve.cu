@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <ctime>
 
 #include "spk_internal.cuh"
@@ -363,58 +364,92 @@ __global__ void __launch_bounds__(32) k_segment_solve(SegArgs A) {
 // rows [32j, 32j+32); a task covers its tiles from the one holding hi-1 down to
 // the one holding lo, with the rows outside [lo, hi) masked.  The tile's slots
 // are contiguous (32 x width values and columns, 128/256-byte aligned), so each
-// tile is one pair of bulk copies with no alignment slack, lanes read their
-// slots conflict-free, and every lane runs the same number of slot steps.
+// tile is one set of bulk copies with no alignment slack, lanes read their slots
+// conflict-free, and every lane runs the same number of slot steps.
+//
+// K right-hand sides are solved together (column-major, leading dimensions ldb /
+// ldx, n for the internal buffers): the matrix slice is read once, each lane
+// keeps K accumulators, and a chain step broadcasts K independent values, so a
+// step costs about the latency of one.  T is the arithmetic/storage type of the
+// matrix and internal vectors (double, or float for the mixed-precision solve);
+// the right-hand side is read as FP64 and converted, the output type is TO.
 
 constexpr int kEllCap = 20;  // staged slots per row; wider tiles are read from global memory
 
-struct TileSmem {
-    alignas(128) double v[2][kEllCap * 32];
+template <int K, typename T>
+struct TileCfg {
+    static constexpr int kWinR = K == 1 ? 128 : 64;           // solved rows kept per right-hand side
+    static constexpr int kChunk = K == 1 ? 8 : (K <= 4 ? 4 : 2);  // slots per load-first chunk
+    static constexpr int kPart = K == 1 ? 4 : 1;               // partial sums per right-hand side
+};
+
+template <int K, typename T>
+struct TileSmemK {
+    alignas(128) T v[2][kEllCap * 32];
     alignas(128) int c[2][kEllCap * 32];
-    alignas(128) double rd[2][32];     // 1 / diagonal of the tile's rows
-    alignas(16) double coef[33][32];   // [tile column i][lane row l] = a(l, i) / a(i, i); row 32: scratch
-    double win[kWin];                  // x of the last kWin solved rows, by row mod kWin
+    alignas(128) T rd[2][32];        // 1 / diagonal of the tile's rows
+    alignas(16) T coef[33][32];      // [tile column i][lane row l] = a(l, i) / a(i, i); row 32: scratch
+    T win[K][TileCfg<K, T>::kWinR];  // x of the last solved rows, by row mod kWinR
     alignas(8) unsigned long long bar[2];
 };
 
-// Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and, when it
-// is at most kEllCap slots wide, its values and columns.
-__device__ __forceinline__ void stage_ell(const SegArgs &A, TileSmem &S, int slot, int j, int e0, int e1) {
-    const unsigned ne = (unsigned)min(e1 - e0, kEllCap * 32);  // the first kEllCap slots
+struct TileArgs {
+    const SegTask *tasks;
+    int ntasks;
+    const void *ell_val;  // T
+    const int *ell_col;
+    const int *ell_ptr;
+    const void *rdiag;    // T, padded to whole tiles
+    int n;
+    const double *rhs;    // caller order, column-major
+    long long ldb;
+    int rev_in;
+    const void *xfix;     // T, U order, column-major with leading dimension n (FULL mode)
+    void *xout;           // TO
+    long long ldx;
+    int rev_out;
+    int *err;
+};
+
+// Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and its first
+// kEllCap slots of values and columns.
+template <typename T, typename S_>
+__device__ __forceinline__ void stage_ell(const TileArgs &A, S_ &S, int slot, int j, int e0, int e1) {
+    const unsigned ne = (unsigned)min(e1 - e0, kEllCap * 32);
     fence_proxy_async();
-    mbar_arrive_expect_tx(&S.bar[slot], 256u + ne * 12u);
-    bulk_g2s(S.rd[slot], A.rdiag + 32ll * j, 256u, &S.bar[slot]);
+    mbar_arrive_expect_tx(&S.bar[slot], 32u * sizeof(T) + ne * (unsigned)(sizeof(T) + 4));
+    bulk_g2s(S.rd[slot], (const T *)A.rdiag + 32ll * j, 32u * sizeof(T), &S.bar[slot]);
     if (ne) {
-        bulk_g2s(S.v[slot], A.ell_val + e0, ne * 8u, &S.bar[slot]);
+        bulk_g2s(S.v[slot], (const T *)A.ell_val + e0, ne * (unsigned)sizeof(T), &S.bar[slot]);
         bulk_g2s(S.c[slot], A.ell_col + e0, ne * 4u, &S.bar[slot]);
     }
 }
 
-template <bool FULL>
-__device__ __forceinline__ double tile_solved_x(const SegArgs &A, const TileSmem &S, int c, int top, int hi_ext) {
-    if (c < hi_ext) {
-        if (c < top + kWin) return S.win[c & (kWin - 1)];
-        return A.xout[A.rev_out ? A.n - 1 - c : c];
-    }
-    return FULL ? A.xfix[c] : 0.0;
-}
-
-template <bool FULL>
-__device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int lo, int hi, int hi_ext) {
+template <bool FULL, int K, typename T, typename TO>
+__device__ bool tile_range(const TileArgs &A, TileSmemK<K, T> &S, unsigned &phase, int lo, int hi, int hi_ext) {
+    using C = TileCfg<K, T>;
+    constexpr int W = C::kWinR, CH = C::kChunk, NP = C::kPart;
     const unsigned FULLMASK = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     if (hi <= lo) return true;
     const int n = A.n;
+    const T *evg = (const T *)A.ell_val;
+    const T *xfix = (const T *)A.xfix;
+    TO *xout = (TO *)A.xout;
     const int jt = (hi - 1) >> 5, jb = lo >> 5;
     const int ntiles = jt - jb + 1;
-    auto load_rhs = [&](int j) {
-        const int r = 32 * j + lane;
-        return (r >= lo && r < hi) ? A.rhs[A.rev_in ? n - 1 - r : r] : 0.0;
+    auto load_rhs = [&](int j, T (&r)[K]) {
+        const int row = 32 * j + lane;
+        const bool ok = row >= lo && row < hi;
+        const long long o = A.rev_in ? n - 1 - row : row;
+#pragma unroll
+        for (int k = 0; k < K; k++) r[k] = ok ? (T)A.rhs[k * A.ldb + o] : T(0);
     };
     int p_hi = A.ell_ptr[jt + 1], p_lo = A.ell_ptr[jt];
     int p_next = ntiles > 1 ? A.ell_ptr[jt - 1] : 0;
-    double rhs_c = load_rhs(jt);
-    if (lane == 0) stage_ell(A, S, 0, jt, p_lo, p_hi);
+    T rhs_c[K];
+    load_rhs(jt, rhs_c);
+    if (lane == 0) stage_ell<T>(A, S, 0, jt, p_lo, p_hi);
     for (int it = 0; it < ntiles; it++) {
         const int j = jt - it;
         const int slot = it & 1;
@@ -422,10 +457,12 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         const int a0 = max(lo, row0), a1 = min(hi, row0 + 32);
         // stage tile j-1, prefetch its right-hand side and the pointer of tile j-2
         int p_next2 = 0;
-        double rhs_n = 0.0;
+        T rhs_n[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) rhs_n[k] = T(0);
         if (it + 1 < ntiles) {
-            if (lane == 0) stage_ell(A, S, slot ^ 1, j - 1, p_next, p_lo);
-            rhs_n = load_rhs(j - 1);
+            if (lane == 0) stage_ell<T>(A, S, slot ^ 1, j - 1, p_next, p_lo);
+            load_rhs(j - 1, rhs_n);
             if (it + 2 < ntiles) p_next2 = A.ell_ptr[j - 2];
         }
         {
@@ -440,33 +477,35 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
         }
         const int width = (p_hi - p_lo) >> 5;
         const int nst = min(width, kEllCap);  // staged slots; the rest are read from global memory
-        const double *rdt = S.rd[slot];
+        const T *rdt = S.rd[slot];
         const int row = row0 + lane;
         const bool act = row >= a0 && row < a1;
-        const double rd = rdt[lane];
-        double acc = act ? rhs_c : 0.0;
-        double pacc[4] = {0.0, 0.0, 0.0, 0.0};
+        const T rd = rdt[lane];
+        T acc[K];
+        T pacc[K][NP];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            acc[k] = act ? rhs_c[k] : T(0);
+#pragma unroll
+            for (int p = 0; p < NP; p++) pacc[k][p] = T(0);
+        }
         bool slow = false;
-        // Branch-free slot step: in-tile columns store a(r, c) / a(c, c) into the
-        // coefficient tile (others into the scratch row), columns inside the
-        // shared window are summed; columns beyond the window or past hi_ext are
-        // flagged for the slow pass below.
-        // Slots in chunks of 8: all loads of a chunk are issued before its shared
+        // Slots in chunks: all loads of a chunk are issued before its shared
         // stores (the stores may alias the staged buffers, so loads cannot move
         // past them).  In-tile columns store a(r, c) / a(c, c) into the
         // coefficient tile (others into the scratch row); columns inside the
         // shared window are summed; columns beyond the window or past hi_ext are
         // flagged for the slow pass.
         if (act) {
-            const double *vs = S.v[slot];
+            const T *vs = S.v[slot];
             const int *cs = S.c[slot];
-            const double *vg = A.ell_val + p_lo;
+            const T *vg = evg + p_lo;
             const int *cg = A.ell_col + p_lo;
-            for (int k0 = 0; k0 < width; k0 += 8) {
-                int cr[8];
-                double vr[8];
+            for (int k0 = 0; k0 < width; k0 += CH) {
+                int cr[CH];
+                T vr[CH];
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < CH; u++) {
                     const int k = k0 + u;
                     if (k < nst) {
                         cr[u] = cs[k * 32 + lane];
@@ -476,22 +515,25 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
                         vr[u] = vg[k * 32 + lane];
                     } else {
                         cr[u] = row;  // no-op slot: zero into the row's own (diagonal) position
-                        vr[u] = 0.0;
+                        vr[u] = T(0);
                     }
                 }
-                int ci[8];
-                double rr[8], wr[8];
+                int ci[CH];
+                T rr[CH], wr[CH][K];
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < CH; u++) {
                     ci[u] = cr[u] < a1 ? cr[u] - row0 : 32;
                     rr[u] = rdt[ci[u] & 31];
-                    wr[u] = S.win[cr[u] & (kWin - 1)];
+#pragma unroll
+                    for (int k = 0; k < K; k++) wr[u][k] = S.win[k][cr[u] & (W - 1)];
                 }
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < CH; u++) {
                     S.coef[ci[u]][lane] = vr[u] * rr[u];
-                    const bool in_win = ci[u] == 32 && cr[u] < hi_ext && cr[u] < a1 + kWin;
-                    pacc[u & 3] = in_win ? fma(vr[u], wr[u], pacc[u & 3]) : pacc[u & 3];
+                    const bool in_win = ci[u] == 32 && cr[u] < hi_ext && cr[u] < a1 + W;
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        pacc[k][u % NP] = in_win ? fma(vr[u], wr[u][k], pacc[k][u % NP]) : pacc[k][u % NP];
                     slow = slow || (ci[u] == 32 && !in_win && (FULL || cr[u] < hi_ext));
                 }
             }
@@ -500,75 +542,105 @@ __device__ bool tile_range(const SegArgs &A, TileSmem &S, unsigned &phase, int l
             // columns solved long ago (beyond the window) or fixed by phases 1-2
             for (int k = 0; k < width; k++) {
                 const int c = k < nst ? S.c[slot][k * 32 + lane] : A.ell_col[p_lo + k * 32 + lane];
-                const double v = k < nst ? S.v[slot][k * 32 + lane] : A.ell_val[p_lo + k * 32 + lane];
+                const T v = k < nst ? S.v[slot][k * 32 + lane] : evg[p_lo + k * 32 + lane];
                 if (c < a1) continue;
                 if (c < hi_ext) {
-                    if (c >= a1 + kWin) pacc[2] = fma(v, A.xout[A.rev_out ? n - 1 - c : c], pacc[2]);
+                    if (c >= a1 + W) {
+                        const long long o = A.rev_out ? n - 1 - c : c;
+#pragma unroll
+                        for (int q = 0; q < K; q++) pacc[q][0] = fma(v, (T)xout[q * A.ldx + o], pacc[q][0]);
+                    }
                 } else if (FULL) {
-                    pacc[3] = fma(v, A.xfix[c], pacc[3]);
+#pragma unroll
+                    for (int q = 0; q < K; q++) pacc[q][0] = fma(v, xfix[(long long)q * n + c], pacc[q][0]);
                 }
             }
         }
-        acc -= (pacc[0] + pacc[1]) + (pacc[2] + pacc[3]);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if constexpr (NP == 4)
+                acc[k] -= (pacc[k][0] + pacc[k][1]) + (pacc[k][2] + pacc[k][3]);
+            else
+                acc[k] -= pacc[k][0];
+        }
         __syncwarp();
-        // in-tile triangle over the active rows (bottom-up); a lane's accumulator
-        // is final after its own step
+        // in-tile triangle over the active rows (bottom-up); a lane's accumulators
+        // are final after its own step
         const int i_hi = a1 - 1 - row0, i_lo = a0 - row0;
         if (i_hi == 31 && i_lo == 0) {
 #pragma unroll
             for (int i = 31; i >= 0; i--) {
-                const double ci = S.coef[i][lane];
-                const double ai = __shfl_sync(FULLMASK, acc, i);
-                acc = fma(-ci, ai, acc);
+                const T ci = S.coef[i][lane];
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const T ai = __shfl_sync(FULLMASK, acc[k], i);
+                    acc[k] = fma(-ci, ai, acc[k]);
+                }
             }
         } else {
             for (int i = i_hi; i >= i_lo; i--) {
-                const double ci = S.coef[i][lane];
-                const double ai = __shfl_sync(FULLMASK, acc, i);
-                acc = fma(-ci, ai, acc);
+                const T ci = S.coef[i][lane];
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const T ai = __shfl_sync(FULLMASK, acc[k], i);
+                    acc[k] = fma(-ci, ai, acc[k]);
+                }
             }
         }
-        const double myx = acc * rd;
         // leave the coefficient tile zero for the next tile
 #pragma unroll
-        for (int i = 0; i < 32; i++) S.coef[i][lane] = 0.0;
+        for (int i = 0; i < 32; i++) S.coef[i][lane] = T(0);
         if (act) {
-            A.xout[A.rev_out ? n - 1 - row : row] = myx;
-            S.win[row & (kWin - 1)] = myx;
+            const long long o = A.rev_out ? n - 1 - row : row;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const T xv = acc[k] * rd;
+                xout[k * A.ldx + o] = (TO)xv;
+                S.win[k][row & (W - 1)] = xv;
+            }
         }
         __syncwarp();
         p_hi = p_lo;
         p_lo = p_next;
         p_next = p_next2;
-        rhs_c = rhs_n;
+#pragma unroll
+        for (int k = 0; k < K; k++) rhs_c[k] = rhs_n[k];
     }
     return true;
 }
 
-__device__ void tile_copy_rows(const SegArgs &A, TileSmem &S, int lo, int hi) {
+// Copy rows [lo, hi) of the phase-1 values into the output and the window.
+template <int K, typename T, typename TO>
+__device__ void tile_copy_rows(const TileArgs &A, TileSmemK<K, T> &S, int lo, int hi) {
+    constexpr int W = TileCfg<K, T>::kWinR;
     const int lane = threadIdx.x & 31;
+    const T *xfix = (const T *)A.xfix;
+    TO *xout = (TO *)A.xout;
     for (int r0 = lo; r0 < hi; r0 += 32 * 8) {
-        double v[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int r = r0 + 32 * u + lane;
-            v[u] = r < hi ? A.xfix[r] : 0.0;
-        }
+        for (int k = 0; k < K; k++) {
+            T v[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int r = r0 + 32 * u + lane;
-            if (r < hi) {
-                A.xout[A.rev_out ? A.n - 1 - r : r] = v[u];
-                if (r < lo + kWin) S.win[r & (kWin - 1)] = v[u];
+            for (int u = 0; u < 8; u++) {
+                const int r = r0 + 32 * u + lane;
+                v[u] = r < hi ? xfix[(long long)k * A.n + r] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int r = r0 + 32 * u + lane;
+                if (r < hi) {
+                    xout[k * A.ldx + (A.rev_out ? A.n - 1 - r : r)] = (TO)v[u];
+                    if (r < lo + W) S.win[k][r & (W - 1)] = v[u];
+                }
             }
         }
     }
     __syncwarp();
 }
 
-template <bool FULL>
-__global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
-    __shared__ TileSmem S;
+template <bool FULL, int K, typename T, typename TO>
+__global__ void __launch_bounds__(32) k_tile_solve(TileArgs A) {
+    __shared__ TileSmemK<K, T> S;
     const int task = blockIdx.x;
     if (task >= A.ntasks) return;
     const int lane = threadIdx.x;
@@ -578,17 +650,48 @@ __global__ void __launch_bounds__(32) k_tile_solve(SegArgs A) {
         fence_mbar_init();
     }
 #pragma unroll
-    for (int i = 0; i < 33; i++) S.coef[i][lane] = 0.0;
+    for (int i = 0; i < 33; i++) S.coef[i][lane] = T(0);
     __syncwarp();
     unsigned phase = 0u;
     const SegTask t = A.tasks[task];
-    if (FULL && t.tail > t.hi) tile_copy_rows(A, S, t.hi, t.tail);
+    if (FULL && t.tail > t.hi) tile_copy_rows<K, T, TO>(A, S, t.hi, t.tail);
     if (t.skip_hi > t.skip_lo) {
-        if (!tile_range<FULL>(A, S, phase, t.skip_hi, t.hi, t.hi)) return;
-        tile_copy_rows(A, S, t.skip_lo, t.skip_hi);
-        tile_range<FULL>(A, S, phase, t.lo, t.skip_lo, t.hi);
+        if (!tile_range<FULL, K, T, TO>(A, S, phase, t.skip_hi, t.hi, t.hi)) return;
+        tile_copy_rows<K, T, TO>(A, S, t.skip_lo, t.skip_hi);
+        tile_range<FULL, K, T, TO>(A, S, phase, t.lo, t.skip_lo, t.hi);
     } else {
-        tile_range<FULL>(A, S, phase, t.lo, t.hi, t.hi);
+        tile_range<FULL, K, T, TO>(A, S, phase, t.lo, t.hi, t.hi);
+    }
+}
+
+// sliced-ELL construction: widths per tile, then slots (padding: value 0, column = row)
+__global__ void k_ell_width(int n, const int *__restrict__ ia, int *__restrict__ width) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
+    int w = len;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if ((threadIdx.x & 31) == 0 && (r >> 5) < (n + 31) / 32) width[r >> 5] = w * 32;
+}
+
+__global__ void k_ell_fill(int n, int ntiles, const int *__restrict__ ia, const int *__restrict__ ja,
+                           const double *__restrict__ a, const int *__restrict__ ptr, double *__restrict__ ev,
+                           int *__restrict__ ec) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = r >> 5, l = r & 31;
+    if (j >= ntiles) return;
+    const int width = (ptr[j + 1] - ptr[j]) >> 5;
+    const int b = r < n ? ia[r] + 1 : 0, len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
+    const int self = r < n ? r : n - 1;
+    for (int k = 0; k < width; k++) {
+        const long long o = (long long)ptr[j] + 32 * k + l;
+        if (k < len) {
+            ev[o] = a[b + k];
+            ec[o] = ja[b + k];
+        } else {
+            ev[o] = 0.0;
+            ec[o] = self;
+        }
     }
 }
 
@@ -632,35 +735,117 @@ __global__ void k_aux_first(int rows, int ncols, const double *__restrict__ W, d
     if (s > tau) atomicMin(first, r);
 }
 
-// sliced-ELL construction: widths per tile, then slots (padding: value 0, column = row)
-__global__ void k_ell_width(int n, const int *__restrict__ ia, int *__restrict__ width) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const int len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
-    int w = len;
+// ---- batched solve support --------------------------------------------------------
+
+// Reduced solve on the kept rows for K right-hand sides stored in T with FP64
+// accumulation (same level structure as k_reduced_solve).
+template <int K, typename T>
+__global__ void __launch_bounds__(1024)
+k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
+                  const int *__restrict__ mapRedX, const int *__restrict__ IT, const int *__restrict__ JT,
+                  const double *__restrict__ Tv, T *__restrict__ xbuf, int n) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int li = 0; li < nlvl; li++) {
+        for (int q = lvl_off[li] + warp; q < lvl_off[li + 1]; q += nwarps) {
+            const int kr = rows[q];
+            double sum[K];
 #pragma unroll
-    for (int o = 16; o; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
-    if ((threadIdx.x & 31) == 0 && (r >> 5) < (n + 31) / 32) width[r >> 5] = w * 32;
+            for (int k = 0; k < K; k++) sum[k] = 0.0;
+            for (int j = IT[kr] + lane; j < IT[kr + 1]; j += 32) {
+                const int c = mapRedX[JT[j]];
+#pragma unroll
+                for (int k = 0; k < K; k++) sum[k] = fma(Tv[j], (double)xbuf[(long long)k * n + c], sum[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+#pragma unroll
+                for (int o = 16; o; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+            }
+            if (lane == 0) {
+                const long long r = mapRedX[kr];
+#pragma unroll
+                for (int k = 0; k < K; k++) xbuf[k * (long long)n + r] = (T)((double)xbuf[k * (long long)n + r] - sum[k]);
+            }
+        }
+        __syncthreads();
+    }
 }
 
-__global__ void k_ell_fill(int n, int ntiles, const int *__restrict__ ia, const int *__restrict__ ja,
-                           const double *__restrict__ a, const int *__restrict__ ptr, double *__restrict__ ev,
-                           int *__restrict__ ec) {
+// R = B - A X in FP64 on the ELL copy (plus the diagonal), in the caller's order
+// (rev: caller row i is U row n-1-i).  One thread per row; a warp covers a tile.
+template <int K>
+__global__ void k_residual(int n, const int *__restrict__ ptr, const double *__restrict__ ev,
+                           const int *__restrict__ ec, const double *__restrict__ diag,
+                           const double *__restrict__ X, long long ldx, const double *__restrict__ B,
+                           long long ldb, double *__restrict__ R, long long ldr, int rev) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = r >> 5, l = r & 31;
-    if (j >= ntiles) return;
-    const int width = (ptr[j + 1] - ptr[j]) >> 5;
-    const int b = r < n ? ia[r] + 1 : 0, len = r < n ? ia[r + 1] - ia[r] - 1 : 0;
-    const int self = r < n ? r : n - 1;
-    for (int k = 0; k < width; k++) {
-        const long long o = (long long)ptr[j] + 32 * k + l;
-        if (k < len) {
-            ev[o] = a[b + k];
-            ec[o] = ja[b + k];
-        } else {
-            ev[o] = 0.0;
-            ec[o] = self;
-        }
+    if (r >= n) return;
+    const int j = r >> 5;
+    const int w = (ptr[j + 1] - ptr[j]) >> 5;
+    const long long base = ptr[j] + (r & 31);
+    const long long orow = rev ? n - 1 - r : r;
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = diag[r] * X[k * ldx + orow];
+    for (int q = 0; q < w; q++) {
+        const int c = ec[base + 32ll * q];
+        const double v = ev[base + 32ll * q];
+        const long long oc = rev ? n - 1 - c : c;
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[k] = fma(v, X[k * ldx + oc], acc[k]);
     }
+#pragma unroll
+    for (int k = 0; k < K; k++) R[k * ldr + orow] = B[k * ldb + orow] - acc[k];
+}
+
+// Per right-hand side: max |R|, max |X|, max |B| (bit patterns of non-negative
+// doubles order like the values, so an integer max is exact).
+__global__ void k_norms(int n, int nrhs, const double *__restrict__ R, long long ldr, const double *__restrict__ X,
+                        long long ldx, const double *__restrict__ B, long long ldb,
+                        unsigned long long *__restrict__ out) {
+    const int k = blockIdx.y;
+    double mr = 0, mx = 0, mb = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        mr = fmax(mr, fabs(R[k * ldr + i]));
+        mx = fmax(mx, fabs(X[k * ldx + i]));
+        mb = fmax(mb, fabs(B[k * ldb + i]));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[3 * k + 0], __double_as_longlong(mr));
+        atomicMax(&out[3 * k + 1], __double_as_longlong(mx));
+        atomicMax(&out[3 * k + 2], __double_as_longlong(mb));
+    }
+}
+
+// X += D (D column-major with leading dimension n)
+__global__ void k_axpy(int n, int nrhs, const double *__restrict__ D, double *__restrict__ X, long long ldx) {
+    const int k = blockIdx.y;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        X[k * ldx + i] += D[k * (long long)n + i];
+}
+
+__global__ void k_to_float(long long count, const double *__restrict__ src, float *__restrict__ dst) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+__global__ void k_diag_rowsum(int n, const int *__restrict__ ia, const double *__restrict__ a,
+                              double *__restrict__ diag, unsigned long long *__restrict__ anorm) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double s = 0.0;
+    if (r < n) {
+        diag[r] = a[ia[r]];
+        for (int q = ia[r]; q < ia[r + 1]; q++) s += fabs(a[q]);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(anorm, __double_as_longlong(s));
 }
 
 __global__ void k_reciprocal_diag(int n, const int *__restrict__ ia, const double *__restrict__ a,
@@ -947,6 +1132,146 @@ int solve_prepare(spk_system *s) {
     return SPK_OK;
 }
 
+namespace {
+
+// One Spike solve of K right-hand sides with the tile solver: phase 1 into the
+// U-order work buffer (T, leading dimension n), the kept reduced rows, phase 3+4
+// into xo (FP64, caller order).
+template <int K, typename T>
+int launch_tiles(spk_system *s, const double *rhs, long long ldb, double *xo, long long ldx, T *work,
+                 cudaStream_t st, bool prof, int ring) {
+    TileArgs A{};
+    A.ell_val = sizeof(T) == 8 ? (const void *)s->ell_val.p : (const void *)s->ell_valf.p;
+    A.ell_col = s->ell_col.p;
+    A.ell_ptr = s->ell_ptr.p;
+    A.rdiag = sizeof(T) == 8 ? (const void *)s->rdiag.p : (const void *)s->rdiagf.p;
+    A.n = s->n;
+    A.rhs = rhs;
+    A.ldb = ldb;
+    A.rev_in = s->uplo == 'L';
+    A.err = s->d_err.p;
+    if (s->redNec && s->ntasks1) {
+        A.tasks = s->d_tasks1.p;
+        A.ntasks = s->ntasks1;
+        A.xfix = nullptr;
+        A.xout = work;
+        A.ldx = s->n;
+        A.rev_out = 0;
+        k_tile_solve<false, K, T, T><<<s->ntasks1, 32, 0, st>>>(A);
+        SPK_CUDA(cudaGetLastError());
+        s->launches++;
+    }
+    if (prof) cudaEventRecord(s->ev[ring][1], st);
+    if (s->redNec && s->nkept) {
+        k_reduced_solve_k<K, T><<<1, 1024, 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
+                                                     s->IT.p, s->JT.p, s->T.p, work, s->n);
+        SPK_CUDA(cudaGetLastError());
+        s->launches++;
+    }
+    if (prof) cudaEventRecord(s->ev[ring][2], st);
+    A.tasks = s->d_tasks2.p;
+    A.ntasks = s->ntasks2;
+    A.xfix = work;
+    A.xout = xo;
+    A.ldx = ldx;
+    A.rev_out = s->uplo == 'L';
+    k_tile_solve<true, K, T, double><<<s->ntasks2, 32, 0, st>>>(A);
+    SPK_CUDA(cudaGetLastError());
+    s->launches++;
+    return SPK_OK;
+}
+
+template <typename T>
+int launch_tiles_k(spk_system *s, int K, const double *rhs, long long ldb, double *xo, long long ldx, T *work,
+                   cudaStream_t st) {
+    switch (K) {
+        case 1: return launch_tiles<1, T>(s, rhs, ldb, xo, ldx, work, st, false, 0);
+        case 2: return launch_tiles<2, T>(s, rhs, ldb, xo, ldx, work, st, false, 0);
+        case 4: return launch_tiles<4, T>(s, rhs, ldb, xo, ldx, work, st, false, 0);
+        case 8: return launch_tiles<8, T>(s, rhs, ldb, xo, ldx, work, st, false, 0);
+        case 16: return launch_tiles<16, T>(s, rhs, ldb, xo, ldx, work, st, false, 0);
+    }
+    set_error(SPK_ERR_ARG, "unsupported batch width %d", K);
+    return SPK_ERR_ARG;
+}
+
+int ensure_work(spk_system *s, size_t bytes) {
+    if (s->work.n >= bytes) return SPK_OK;
+    return s->work.alloc(bytes);
+}
+
+// float copies of the ELL values and diagonal reciprocals (mixed-precision solve)
+int ensure_fp32(spk_system *s) {
+    if (s->ell_valf.p) return SPK_OK;
+    const long long ne = std::max<long long>(s->ell_entries, 1), nr = s->rdiag.n;
+    SPK_TRY(s->ell_valf.alloc(ne));
+    SPK_TRY(s->rdiagf.alloc(nr));
+    k_to_float<<<1184, 256, 0, s->stream>>>(s->ell_entries, s->ell_val.p, s->ell_valf.p);
+    k_to_float<<<1184, 256, 0, s->stream>>>(nr, s->rdiag.p, s->rdiagf.p);
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return SPK_OK;
+}
+
+// FP64 diagonal and ||A||_inf for residuals
+int ensure_residual(spk_system *s) {
+    if (s->diag.p) return SPK_OK;
+    SPK_TRY(s->diag.alloc(s->n));
+    DBuf<unsigned long long> an;
+    SPK_TRY(an.alloc(1));
+    SPK_CUDA(cudaMemsetAsync(an.p, 0, sizeof(unsigned long long), s->stream));
+    k_diag_rowsum<<<blocks_for(s->n), 256, 0, s->stream>>>(s->n, s->uia.p, s->ua.p, s->diag.p, an.p);
+    SPK_CUDA(cudaGetLastError());
+    unsigned long long h = 0;
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    SPK_CUDA(cudaMemcpy(&h, an.p, sizeof(h), cudaMemcpyDeviceToHost));
+    memcpy(&s->anorm, &h, sizeof(double));
+    SPK_TRY(s->d_norms.alloc(3 * 16));
+    return SPK_OK;
+}
+
+template <int K>
+void launch_residual(spk_system *s, const double *X, long long ldx, const double *B, long long ldb, double *R,
+                     long long ldr, cudaStream_t st) {
+    k_residual<K><<<blocks_for(s->n), 256, 0, st>>>(s->n, s->ell_ptr.p, s->ell_val.p, s->ell_col.p, s->diag.p, X, ldx,
+                                                     B, ldb, R, ldr, s->uplo == 'L');
+}
+
+void residual_k(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
+                long long ldr, cudaStream_t st) {
+    switch (K) {
+        case 1: launch_residual<1>(s, X, ldx, B, ldb, R, ldr, st); break;
+        case 2: launch_residual<2>(s, X, ldx, B, ldb, R, ldr, st); break;
+        case 4: launch_residual<4>(s, X, ldx, B, ldb, R, ldr, st); break;
+        case 8: launch_residual<8>(s, X, ldx, B, ldb, R, ldr, st); break;
+        default: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
+    }
+}
+
+// max over the K right-hand sides of ||R||_inf / (||A||_inf ||X||_inf + ||B||_inf)
+int scaled_residual(spk_system *s, int K, const double *R, long long ldr, const double *X, long long ldx,
+                    const double *B, long long ldb, cudaStream_t st, double *out) {
+    SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
+    k_norms<<<dim3(64, K), 256, 0, st>>>(s->n, K, R, ldr, X, ldx, B, ldb, s->d_norms.p);
+    SPK_CUDA(cudaGetLastError());
+    unsigned long long h[48];
+    SPK_CUDA(cudaMemcpyAsync(h, s->d_norms.p, sizeof(unsigned long long) * 3 * K, cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    double worst = 0.0;
+    for (int k = 0; k < K; k++) {
+        double nr, nx, nb;
+        memcpy(&nr, &h[3 * k], 8);
+        memcpy(&nx, &h[3 * k + 1], 8);
+        memcpy(&nb, &h[3 * k + 2], 8);
+        const double den = s->anorm * nx + nb;
+        worst = std::max(worst, den > 0 ? nr / den : nr);
+    }
+    *out = worst;
+    return SPK_OK;
+}
+
+}  // namespace
+
 int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph) {
     if (!s->built) {
         set_error(SPK_ERR_STATE, "no preprocessed system");
@@ -968,54 +1293,151 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         if (s->ev_pending[ring]) SPK_TRY(collect_event_set(s, ring));
         cudaEventRecord(s->ev[ring][0], st);
     }
-    SegArgs A;
-    A.ia = s->uia.p;
-    A.ja = s->uja.p;
-    A.a = s->ua.p;
-    A.rdiag = s->rdiag.p;
-    A.ell_val = s->ell_val.p;
-    A.ell_col = s->ell_col.p;
-    A.ell_ptr = s->ell_ptr.p;
-    A.n = s->n;
-    A.rhs = b;
-    A.rev_in = s->uplo == 'L';
-    A.err = s->d_err.p;
-    if (s->redNec && s->ntasks1) {
-        A.tasks = s->d_tasks1.p;
-        A.ntasks = s->ntasks1;
-        A.xfix = nullptr;
-        A.xout = s->xbuf.p;
-        A.rev_out = 0;
-        if (s->ell_ok) k_tile_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
-        else k_segment_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
+    if (s->ell_ok && !ph) {
+        SPK_TRY((launch_tiles<1, double>(s, b, s->n, x, s->n, s->xbuf.p, st, prof, ring)));
+    } else {
+        // CSR segment solver (or the timed legacy path, which times the phases)
+        SegArgs A;
+        A.ia = s->uia.p;
+        A.ja = s->uja.p;
+        A.a = s->ua.p;
+        A.rdiag = s->rdiag.p;
+        A.n = s->n;
+        A.rhs = b;
+        A.rev_in = s->uplo == 'L';
+        A.err = s->d_err.p;
+        TileArgs TA{};
+        TA.ell_val = s->ell_val.p;
+        TA.ell_col = s->ell_col.p;
+        TA.ell_ptr = s->ell_ptr.p;
+        TA.rdiag = s->rdiag.p;
+        TA.n = s->n;
+        TA.rhs = b;
+        TA.ldb = s->n;
+        TA.rev_in = s->uplo == 'L';
+        TA.err = s->d_err.p;
+        if (s->redNec && s->ntasks1) {
+            A.tasks = TA.tasks = s->d_tasks1.p;
+            A.ntasks = TA.ntasks = s->ntasks1;
+            A.xfix = nullptr;
+            TA.xfix = nullptr;
+            A.xout = s->xbuf.p;
+            TA.xout = s->xbuf.p;
+            TA.ldx = s->n;
+            A.rev_out = TA.rev_out = 0;
+            if (s->ell_ok) k_tile_solve<false, 1, double, double><<<s->ntasks1, 32, 0, st>>>(TA);
+            else k_segment_solve<false><<<s->ntasks1, 32, 0, st>>>(A);
+            SPK_CUDA(cudaGetLastError());
+            s->launches++;
+        }
+        if (prof) cudaEventRecord(s->ev[ring][1], st);
+        lap(1);
+        if (s->redNec && s->nkept) {
+            k_reduced_solve<<<1, 1024, 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p, s->IT.p,
+                                                s->JT.p, s->T.p, s->xbuf.p);
+            SPK_CUDA(cudaGetLastError());
+            s->launches++;
+        }
+        if (prof) cudaEventRecord(s->ev[ring][2], st);
+        lap(2);
+        A.tasks = TA.tasks = s->d_tasks2.p;
+        A.ntasks = TA.ntasks = s->ntasks2;
+        A.xfix = s->xbuf.p;
+        TA.xfix = s->xbuf.p;
+        A.xout = x;
+        TA.xout = x;
+        TA.ldx = s->n;
+        A.rev_out = TA.rev_out = s->uplo == 'L';
+        if (s->ell_ok) k_tile_solve<true, 1, double, double><<<s->ntasks2, 32, 0, st>>>(TA);
+        else k_segment_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
         SPK_CUDA(cudaGetLastError());
         s->launches++;
     }
-    if (prof) cudaEventRecord(s->ev[ring][1], st);
-    lap(1);
-    if (s->redNec && s->nkept) {
-        k_reduced_solve<<<1, 1024, 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p, s->IT.p,
-                                            s->JT.p, s->T.p, s->xbuf.p);
-        SPK_CUDA(cudaGetLastError());
-        s->launches++;
-    }
-    if (prof) cudaEventRecord(s->ev[ring][2], st);
-    lap(2);
-    A.tasks = s->d_tasks2.p;
-    A.ntasks = s->ntasks2;
-    A.xfix = s->xbuf.p;
-    A.xout = x;
-    A.rev_out = s->uplo == 'L';
-    if (s->ell_ok) k_tile_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
-    else k_segment_solve<true><<<s->ntasks2, 32, 0, st>>>(A);
-    SPK_CUDA(cudaGetLastError());
-    s->launches++;
     if (prof) {
         cudaEventRecord(s->ev[ring][3], st);
         s->ev_pending[ring] = 1;
         s->ev_next++;
     }
     lap(3);
+    return SPK_OK;
+}
+
+// Batched solve of nrhs right-hand sides (device, column-major).  mode 0: FP64
+// tile solves in groups of up to 16.  mode 1: FP32 tile solves with FP64
+// residuals R = B - A X and FP64 correction updates X += solve32(R), iterated
+// until the scaled residual is <= tol (tol < 0: exactly maxit corrections, no
+// host synchronisation).
+int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
+                double tol, int maxit, cudaStream_t st, int *iters, double *resid) {
+    if (!s->built) {
+        set_error(SPK_ERR_STATE, "no preprocessed system");
+        return SPK_ERR_STATE;
+    }
+    if (nrhs <= 0 || ldb < s->n || ldx < s->n || (mode != 0 && mode != 1)) {
+        set_error(SPK_ERR_ARG, "invalid batch arguments (nrhs=%d, ldb=%lld, ldx=%lld, mode=%d)", nrhs, ldb, ldx, mode);
+        return SPK_ERR_ARG;
+    }
+    if (!s->ell_ok) {
+        if (mode != 0) {
+            set_error(SPK_ERR_ARG, "the mixed-precision batch needs the sliced-ELL layout");
+            return SPK_ERR_ARG;
+        }
+        for (int k = 0; k < nrhs; k++) SPK_TRY(solve(s, B + k * ldb, X + k * ldx, st, nullptr));
+        if (iters) *iters = 0;
+        return SPK_OK;
+    }
+    const long long n = s->n;
+    int max_it = 0;
+    double worst = 0.0;
+    if (mode == 1) {
+        SPK_TRY(ensure_fp32(s));
+        SPK_TRY(ensure_residual(s));
+        if (s->rbuf.n < (size_t)(16 * n)) SPK_TRY(s->rbuf.alloc(16 * n));
+        if (s->dbuf.n < (size_t)(16 * n)) SPK_TRY(s->dbuf.alloc(16 * n));
+    } else if (resid) {
+        SPK_TRY(ensure_residual(s));
+        if (s->rbuf.n < (size_t)(16 * n)) SPK_TRY(s->rbuf.alloc(16 * n));
+    }
+    for (int g = 0; g < nrhs;) {
+        const int left = nrhs - g;
+        const int K = left >= 16 ? 16 : left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+        const double *Bg = B + g * ldb;
+        double *Xg = X + g * ldx;
+        if (mode == 0) {
+            SPK_TRY(ensure_work(s, sizeof(double) * K * n));
+            SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
+            if (resid) {
+                residual_k(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st);
+                double r = 0;
+                SPK_TRY(scaled_residual(s, K, s->rbuf.p, n, Xg, ldx, Bg, ldb, st, &r));
+                worst = std::max(worst, r);
+            }
+        } else {
+            SPK_TRY(ensure_work(s, sizeof(float) * K * n));
+            float *wk = (float *)s->work.p;
+            SPK_TRY(launch_tiles_k<float>(s, K, Bg, ldb, Xg, ldx, wk, st));
+            int it = 0;
+            double r = -1.0;
+            for (;; it++) {
+                const bool check = tol >= 0 || (resid && it == maxit);
+                if (tol < 0 && it == maxit && !resid) break;
+                residual_k(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st);
+                if (check) {
+                    SPK_TRY(scaled_residual(s, K, s->rbuf.p, n, Xg, ldx, Bg, ldb, st, &r));
+                    if ((tol >= 0 && r <= tol) || it == maxit) break;
+                }
+                if (it == maxit) break;
+                SPK_TRY(launch_tiles_k<float>(s, K, s->rbuf.p, n, s->dbuf.p, n, wk, st));
+                k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, s->dbuf.p, Xg, ldx);
+                SPK_CUDA(cudaGetLastError());
+            }
+            max_it = std::max(max_it, it);
+            if (r >= 0) worst = std::max(worst, r);
+        }
+        g += K;
+    }
+    if (iters) *iters = max_it;
+    if (resid) *resid = worst;
     return SPK_OK;
 }
 

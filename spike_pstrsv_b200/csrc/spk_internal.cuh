@@ -135,6 +135,12 @@ struct spk_system {
     spk::DBuf<int> ell_col, ell_ptr;
     int ell_ok = 0;
     long long ell_entries = 0;
+    // batched / mixed-precision solve support (allocated on first use)
+    spk::DBuf<float> ell_valf, rdiagf;
+    spk::DBuf<double> diag, rbuf, dbuf;
+    spk::DBuf<char> work;
+    spk::DBuf<unsigned long long> d_norms;
+    double anorm = 0.0;
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     // optional per-phase device timing (spk_set_profiling)
@@ -155,6 +161,8 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
                char uplo, int flb, const int *starts, const int *ends, int ptr_on_device,
                double *phase_seconds);
 int solve(spk_system *s, const double *b, double *x, cudaStream_t stream, double *phase_seconds);
+int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
+                double tol, int maxit, cudaStream_t stream, int *iters, double *resid);
 int solve_prepare(spk_system *s);
 int check_device_error(spk_system *s);
 int collect_phase_times(spk_system *s);

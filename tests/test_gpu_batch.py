@@ -1,0 +1,71 @@
+"""Batched solves (many right-hand sides per launch) in FP64 and in FP32 with FP64
+iterative refinement, against single solves and the known solutions."""
+import numpy as np
+import pytest
+
+import spike_pstrsv_b200 as spk
+from cases import rel_err
+from spike_pstrsv_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda:0")
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("nrhs", [1, 3, 13, 32])
+def test_batch_fp64_matches_single_solves(uplo, nrhs):
+    L = synth.banded_lower(60000, seed=11)
+    A = L if uplo == "L" else synth.transpose(L)
+    Xt, B = synth.make_rhs(A, seed=5, nrhs=nrhs)
+    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 16, uplo, 1)
+    dB = _dev(B)
+    dX = _dev(np.zeros_like(B))
+    it, r = S.solve_batch(dB, dX, mode=0)
+    X = dX.cpu().numpy()
+    assert r <= 1e-12
+    for k in range(nrhs):
+        assert rel_err(X[k], S.solve(B[k])) <= 1e-13
+        assert rel_err(X[k], Xt[k]) <= 1e-12
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("nrhs", [1, 5, 16])
+def test_batch_fp32_refinement_reaches_fp64_accuracy(uplo, nrhs):
+    L = synth.banded_lower(60000, seed=12)
+    A = L if uplo == "L" else synth.transpose(L)
+    Xt, B = synth.make_rhs(A, seed=6, nrhs=nrhs)
+    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 32, uplo, 1)
+    dB = _dev(B)
+    dX = _dev(np.zeros_like(B))
+    it, r = S.solve_batch(dB, dX, mode=1, tol=1e-12, maxit=8)
+    X = dX.cpu().numpy()
+    assert r <= 1e-12
+    assert 1 <= it <= 4
+    for k in range(nrhs):
+        assert rel_err(X[k], Xt[k]) <= 1e-12
+
+
+def test_batch_fp32_fixed_iterations_and_poisson():
+    L = synth.poisson2d_lower(128)
+    Xt, B = synth.make_rhs(L, seed=0, nrhs=4)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, 4, "L", 1)
+    dB, dX = _dev(B), _dev(np.zeros_like(B))
+    it, r = S.solve_batch(dB, dX, mode=1, tol=-1.0, maxit=3)
+    assert it == 3 and r <= 1e-12
+    assert max(rel_err(dX.cpu().numpy()[k], Xt[k]) for k in range(4)) <= 1e-12
+
+
+def test_batch_rejects_host_arrays_and_bad_leading_dimension():
+    L = synth.poisson2d_lower(16)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, 2, "L", 1)
+    import torch
+    B = torch.zeros((2, L.m), dtype=torch.float64)
+    with pytest.raises(spk.SpkError):
+        S.solve_batch(B, B.clone(), mode=0)
+    dB = torch.zeros((2, L.m - 1), dtype=torch.float64, device="cuda:0")
+    with pytest.raises(spk.SpkError):
+        S.solve_batch(dB, dB.clone(), mode=0)
