@@ -664,6 +664,317 @@ __global__ void __launch_bounds__(32) k_tile_solve(TileArgs A) {
     }
 }
 
+// ---- right-hand-side-parallel tile solver (batches of up to 32) -----------------
+//
+// Lane k owns right-hand side k and walks the rows of the task bottom-up; the
+// row's slots are warp-uniform broadcast loads and there is no cross-lane
+// dependency (no chain broadcast).
+//
+// * A 129-row window in shared memory, indexed [row mod 128][lane], holds x of
+//   the solved rows and, for the tile being solved, its right-hand sides
+//   (written there, coalesced along rows, before the tile's first row; row r's
+//   slot then turns from b_r into x_r).  Writing tile rows row0..row0+31 evicts
+//   rows row0+128.., so the window answers for columns c < row0 + 128 (at least
+//   r + 97); farther columns of the task read the output in global memory.
+//   Window row 128 is zero (padding slots point there).
+// * The next tile's slots are bulk-copied (slot-major, as stored) while the
+//   current tile is solved, then transposed to row-major so that a row's slots
+//   are a few 16-byte broadcast loads.  A tile whose columns all fall inside
+//   the window (the common case) stores window offsets instead of columns and
+//   runs the branch-free path, unrolled for its width class (4, 8, 16 slots)
+//   with the next row's slots loaded ahead.
+// * The next tile's right-hand sides are loaded into registers while the
+//   current tile is solved.  Lanes k >= nk idle (no global access).
+
+constexpr int kRhsWin = 128;  // window rows (power of two)
+constexpr int kRhsCap = 16;   // transposed slots per row; wider tiles run the general path
+constexpr int kRhsLd = 33;    // window row stride (elements)
+
+template <typename T>
+struct RhsSmem {
+    alignas(128) T v[kRhsCap * 32];   // next tile, slot-major
+    alignas(128) int c[kRhsCap * 32];
+    alignas(128) T rdn[32];
+    alignas(16) int rc[33][kRhsCap];  // current tile, row l at l + 1: window offsets (fast) or columns (-1: padding)
+    alignas(16) T rv[33][kRhsCap];
+    T rd[32];
+    T win[kRhsWin + 1][kRhsLd];
+    alignas(8) unsigned long long bar;
+};
+
+template <typename T>
+__device__ __forceinline__ void stage_rhs_tile(const TileArgs &A, RhsSmem<T> &S, int j, int e0, int e1) {
+    const unsigned ne = (unsigned)min(e1 - e0, kRhsCap * 32);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&S.bar, 32u * sizeof(T) + ne * (unsigned)(sizeof(T) + 4));
+    bulk_g2s(S.rdn, (const T *)A.rdiag + 32ll * j, 32u * sizeof(T), &S.bar);
+    if (ne) {
+        bulk_g2s(S.v, (const T *)A.ell_val + e0, ne * (unsigned)sizeof(T), &S.bar);
+        bulk_g2s(S.c, A.ell_col + e0, ne * 4u, &S.bar);
+    }
+}
+
+// Right-hand sides of tile rows [a0, a1) (lane = row), zero elsewhere.
+template <typename T>
+__device__ __forceinline__ void load_rhs_tile(const TileArgs &A, int row0, int a0, int a1, int nk, T (&nb)[32]) {
+    const int row = row0 + (threadIdx.x & 31);
+    const bool ok = row >= a0 && row < a1;
+    const long long o = A.rev_in ? A.n - 1 - row : row;
+#pragma unroll
+    for (int k = 0; k < 32; k++) nb[k] = (ok && k < nk) ? (T)A.rhs[k * A.ldb + o] : T(0);
+}
+
+// x of column c > r for lane's right-hand side: window below wlim, the task's
+// output below hi_ext, the phase-1 values (FULL) or zero beyond.
+template <bool FULL, typename T, typename TO>
+__device__ __forceinline__ T rhs_x(const TileArgs &A, const RhsSmem<T> &S, int c, int wlim, int hi_ext, bool act) {
+    const int lane = threadIdx.x & 31;
+    if (c < wlim) return S.win[c & (kRhsWin - 1)][lane];
+    if (!act) return T(0);
+    if (c < hi_ext) return (T)((const TO *)A.xout)[lane * A.ldx + (A.rev_out ? A.n - 1 - c : c)];
+    return FULL ? ((const T *)A.xfix)[(long long)lane * A.n + c] : T(0);
+}
+
+template <int W, typename T>
+__device__ __forceinline__ void rhs_row_slots(const RhsSmem<T> &S, int lp1, int (&ci)[W], T (&cv)[W]) {
+#pragma unroll
+    for (int i = 0; i < W; i += 4) {
+        const int4 c4 = *reinterpret_cast<const int4 *>(&S.rc[lp1][i]);
+        ci[i] = c4.x;
+        ci[i + 1] = c4.y;
+        ci[i + 2] = c4.z;
+        ci[i + 3] = c4.w;
+    }
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+        for (int i = 0; i < W; i += 2) {
+            const double2 v2 = *reinterpret_cast<const double2 *>(&S.rv[lp1][i]);
+            cv[i] = v2.x;
+            cv[i + 1] = v2.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; i += 4) {
+            const float4 v4 = *reinterpret_cast<const float4 *>(&S.rv[lp1][i]);
+            cv[i] = v4.x;
+            cv[i + 1] = v4.y;
+            cv[i + 2] = v4.z;
+            cv[i + 3] = v4.w;
+        }
+    }
+}
+
+// Rows a1-1 .. a0 of a tile whose slots are window offsets (branch-free).
+template <int W, typename T>
+__device__ __forceinline__ void rhs_rows_fast(RhsSmem<T> &S, int row0, int a0, int a1) {
+    const int lane = threadIdx.x & 31;
+    T *wf = &S.win[0][0];
+    int ci[W];
+    T cv[W];
+    rhs_row_slots<W, T>(S, a1 - row0, ci, cv);
+    for (int r = a1 - 1; r >= a0; r--) {
+        const int l = r - row0;
+        T xv[W];
+#pragma unroll
+        for (int i = 0; i < W; i++) xv[i] = wf[ci[i] + lane];
+        T *wr = wf + (r & (kRhsWin - 1)) * kRhsLd + lane;
+        T p[4] = {*wr, T(0), T(0), T(0)};
+        int ni[W];
+        T nv[W];
+        rhs_row_slots<W, T>(S, l, ni, nv);  // row l - 1 (stored at l); row -1 is the spare row 0
+#pragma unroll
+        for (int i = 0; i < W; i++) p[i & 3] = fma(-cv[i], xv[i], p[i & 3]);
+        *wr = ((p[0] + p[1]) + (p[2] + p[3])) * S.rd[l];
+#pragma unroll
+        for (int i = 0; i < W; i++) {
+            ci[i] = ni[i];
+            cv[i] = nv[i];
+        }
+    }
+}
+
+// Rows a1-1 .. a0 of any tile: columns (slots >= kRhsCap from global memory),
+// window / output / phase-1 lookups per slot.
+template <bool FULL, typename T, typename TO>
+__device__ void rhs_rows_general(const TileArgs &A, RhsSmem<T> &S, int row0, int a0, int a1, int width, int p_lo,
+                                 int wlim, int hi_ext, bool act) {
+    const int lane = threadIdx.x & 31;
+    const int nst = min(width, kRhsCap);
+    const T *vg = (const T *)A.ell_val + p_lo;
+    const int *cg = A.ell_col + p_lo;
+    for (int r = a1 - 1; r >= a0; r--) {
+        const int l = r - row0;
+        T *wr = &S.win[r & (kRhsWin - 1)][lane];
+        T p0 = *wr, p1 = T(0);
+        for (int q = 0; q < width; q++) {
+            const int c = q < nst ? S.rc[l + 1][q] : cg[q * 32 + l];
+            const T v = q < nst ? S.rv[l + 1][q] : vg[q * 32 + l];
+            if (c > r) {
+                if (q & 1) p1 = fma(-v, rhs_x<FULL, T, TO>(A, S, c, wlim, hi_ext, act), p1);
+                else p0 = fma(-v, rhs_x<FULL, T, TO>(A, S, c, wlim, hi_ext, act), p0);
+            }
+        }
+        *wr = (p0 + p1) * S.rd[l];
+    }
+}
+
+template <bool FULL, typename T, typename TO>
+__device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int lo, int hi, int hi_ext, int nk) {
+    const int lane = threadIdx.x & 31;
+    if (hi <= lo) return true;
+    const bool act = lane < nk;
+    const int n = A.n;
+    TO *xout = (TO *)A.xout;
+    const int jt = (hi - 1) >> 5, jb = lo >> 5;
+    const int ntiles = jt - jb + 1;
+    int p_hi = A.ell_ptr[jt + 1], p_lo = A.ell_ptr[jt];
+    int p_next = ntiles > 1 ? A.ell_ptr[jt - 1] : 0;
+    __syncwarp();
+    if (lane == 0) stage_rhs_tile<T>(A, S, jt, p_lo, p_hi);
+    T nb[32];
+    load_rhs_tile<T>(A, 32 * jt, max(lo, 32 * jt), hi, nk, nb);
+    for (int it = 0; it < ntiles; it++) {
+        const int j = jt - it;
+        const int row0 = 32 * j;
+        const int row = row0 + lane;
+        const int a0 = max(lo, row0), a1 = min(hi, row0 + 32);
+        const bool mine = row >= a0 && row < a1;
+        if (mine) {
+            T *w = S.win[row & (kRhsWin - 1)];
+#pragma unroll
+            for (int k = 0; k < 32; k++) w[k] = nb[k];
+        }
+        {
+            const long long t0 = clock64();
+            while (!mbar_try_wait(&S.bar, phase)) {
+                if (clock64() - t0 > kWaitCycles) {
+                    if (lane == 0) atomicExch(A.err, 1);
+                    return false;
+                }
+            }
+            phase ^= 1u;
+        }
+        // transpose the staged tile to row-major (lane = row)
+        const int width = (p_hi - p_lo) >> 5;
+        const int nst = min(width, kRhsCap);
+        const int wlim = min(row0 + kRhsWin, hi_ext);
+        int cl[kRhsCap];
+        T vl[kRhsCap];
+        bool local = true;
+#pragma unroll
+        for (int q = 0; q < kRhsCap; q++) {
+            cl[q] = q < nst ? S.c[q * 32 + lane] : -1;
+            vl[q] = q < nst ? S.v[q * 32 + lane] : T(0);
+            if (cl[q] == row) cl[q] = -1;
+            if (mine && cl[q] >= wlim) local = false;
+        }
+        const bool fast = __all_sync(0xffffffffu, local) && width <= kRhsCap;
+#pragma unroll
+        for (int q = 0; q < kRhsCap; q += 4) {
+            int4 o;
+            int *op = &o.x;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int c = cl[q + u];
+                op[u] = fast ? (c < 0 ? kRhsWin * kRhsLd : (c & (kRhsWin - 1)) * kRhsLd) : c;
+            }
+            *reinterpret_cast<int4 *>(&S.rc[lane + 1][q]) = o;
+        }
+        if constexpr (sizeof(T) == 8) {
+#pragma unroll
+            for (int q = 0; q < kRhsCap; q += 2)
+                *reinterpret_cast<double2 *>(&S.rv[lane + 1][q]) = make_double2(vl[q], vl[q + 1]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < kRhsCap; q += 4)
+                *reinterpret_cast<float4 *>(&S.rv[lane + 1][q]) = make_float4(vl[q], vl[q + 1], vl[q + 2], vl[q + 3]);
+        }
+        S.rd[lane] = S.rdn[lane];
+        __syncwarp();
+        int p_next2 = 0;
+        if (it + 1 < ntiles) {
+            if (lane == 0) stage_rhs_tile<T>(A, S, j - 1, p_next, p_lo);
+            if (it + 2 < ntiles) p_next2 = A.ell_ptr[j - 2];
+            load_rhs_tile<T>(A, row0 - 32, max(lo, row0 - 32), row0, nk, nb);
+        }
+        if (fast) {
+            if (width <= 4) rhs_rows_fast<4, T>(S, row0, a0, a1);
+            else if (width <= 8) rhs_rows_fast<8, T>(S, row0, a0, a1);
+            else rhs_rows_fast<16, T>(S, row0, a0, a1);
+        } else {
+            rhs_rows_general<FULL, T, TO>(A, S, row0, a0, a1, width, p_lo, wlim, hi_ext, act);
+        }
+        __syncwarp();
+        if (mine) {
+            const long long o = A.rev_out ? n - 1 - row : row;
+            const T *w = S.win[row & (kRhsWin - 1)];
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (k < nk) xout[k * A.ldx + o] = (TO)w[k];
+        }
+        __syncwarp();
+        p_hi = p_lo;
+        p_lo = p_next;
+        p_next = p_next2;
+    }
+    return true;
+}
+
+// Copy rows [lo, hi) of the phase-1 values into the output and the window, 32
+// rows (lane = row) by all right-hand sides per step, loads ahead of stores.
+template <typename T, typename TO>
+__device__ void rhs_copy_rows(const TileArgs &A, RhsSmem<T> &S, int lo, int hi, int nk) {
+    const int lane = threadIdx.x & 31;
+    const T *xfix = (const T *)A.xfix;
+    TO *xout = (TO *)A.xout;
+    for (int r0 = lo; r0 < hi; r0 += 32) {
+        const int r = r0 + lane;
+        const bool ok = r < hi;
+        T v[32];
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = (ok && k < nk) ? xfix[(long long)k * A.n + r] : T(0);
+        if (ok) {
+            const long long o = A.rev_out ? A.n - 1 - r : r;
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (k < nk) xout[k * A.ldx + o] = (TO)v[k];
+            if (r < lo + kRhsWin) {
+                T *w = S.win[r & (kRhsWin - 1)];
+#pragma unroll
+                for (int k = 0; k < 32; k++) w[k] = v[k];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+template <bool FULL, typename T, typename TO>
+__global__ void __launch_bounds__(32) k_rhs_solve(TileArgs A, int nk) {
+    __shared__ RhsSmem<T> S;
+    const int task = blockIdx.x;
+    if (task >= A.ntasks) return;
+    const int lane = threadIdx.x;
+    if (lane == 0) {
+        mbar_init(&S.bar, 1);
+        fence_mbar_init();
+    }
+    S.win[kRhsWin][lane] = T(0);
+#pragma unroll
+    for (int q = 0; q < kRhsCap; q += 4) *reinterpret_cast<int4 *>(&S.rc[0][q]) = make_int4(0, 0, 0, 0);
+    if (lane < kRhsCap) S.rv[0][lane] = T(0);
+    __syncwarp();
+    unsigned phase = 0u;
+    const SegTask t = A.tasks[task];
+    if (FULL && t.tail > t.hi) rhs_copy_rows<T, TO>(A, S, t.hi, t.tail, nk);
+    if (t.skip_hi > t.skip_lo) {
+        if (!rhs_range<FULL, T, TO>(A, S, phase, t.skip_hi, t.hi, t.hi, nk)) return;
+        rhs_copy_rows<T, TO>(A, S, t.skip_lo, t.skip_hi, nk);
+        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.skip_lo, t.hi, nk);
+    } else {
+        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.hi, t.hi, nk);
+    }
+}
+
 // sliced-ELL construction: widths per tile, then slots (padding: value 0, column = row)
 __global__ void k_ell_width(int n, const int *__restrict__ ia, int *__restrict__ width) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -739,8 +1050,11 @@ __global__ void k_aux_first(int rows, int ncols, const double *__restrict__ W, d
 
 // Reduced solve on the kept rows for K right-hand sides stored in T with FP64
 // accumulation (same level structure as k_reduced_solve).
+template <int K>
+constexpr int red_threads() { return K >= 16 ? 512 : 1024; }  // K >= 16: registers for the K sums
+
 template <int K, typename T>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(red_threads<K>())
 k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
                   const int *__restrict__ mapRedX, const int *__restrict__ IT, const int *__restrict__ JT,
                   const double *__restrict__ Tv, T *__restrict__ xbuf, int n) {
@@ -1163,7 +1477,7 @@ int launch_tiles(spk_system *s, const double *rhs, long long ldb, double *xo, lo
     }
     if (prof) cudaEventRecord(s->ev[ring][1], st);
     if (s->redNec && s->nkept) {
-        k_reduced_solve_k<K, T><<<1, 1024, 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
+        k_reduced_solve_k<K, T><<<1, red_threads<K>(), 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
                                                      s->IT.p, s->JT.p, s->T.p, work, s->n);
         SPK_CUDA(cudaGetLastError());
         s->launches++;
@@ -1193,6 +1507,48 @@ int launch_tiles_k(spk_system *s, int K, const double *rhs, long long ldb, doubl
     }
     set_error(SPK_ERR_ARG, "unsupported batch width %d", K);
     return SPK_ERR_ARG;
+}
+
+// One Spike solve of nk <= 32 right-hand sides with the right-hand-side-parallel
+// solver; work holds 32 columns (leading dimension n).
+template <typename T>
+int launch_rhs(spk_system *s, int nk, const double *rhs, long long ldb, double *xo, long long ldx, T *work,
+               cudaStream_t st) {
+    TileArgs A{};
+    A.ell_val = sizeof(T) == 8 ? (const void *)s->ell_val.p : (const void *)s->ell_valf.p;
+    A.ell_col = s->ell_col.p;
+    A.ell_ptr = s->ell_ptr.p;
+    A.rdiag = sizeof(T) == 8 ? (const void *)s->rdiag.p : (const void *)s->rdiagf.p;
+    A.n = s->n;
+    A.rhs = rhs;
+    A.ldb = ldb;
+    A.rev_in = s->uplo == 'L';
+    A.err = s->d_err.p;
+    if (s->redNec && s->ntasks1) {
+        A.tasks = s->d_tasks1.p;
+        A.ntasks = s->ntasks1;
+        A.xout = work;
+        A.ldx = s->n;
+        k_rhs_solve<false, T, T><<<s->ntasks1, 32, 0, st>>>(A, nk);
+        SPK_CUDA(cudaGetLastError());
+        s->launches++;
+    }
+    if (s->redNec && s->nkept) {
+        k_reduced_solve_k<32, T><<<1, red_threads<32>(), 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
+                                                      s->IT.p, s->JT.p, s->T.p, work, s->n);
+        SPK_CUDA(cudaGetLastError());
+        s->launches++;
+    }
+    A.tasks = s->d_tasks2.p;
+    A.ntasks = s->ntasks2;
+    A.xfix = work;
+    A.xout = xo;
+    A.ldx = ldx;
+    A.rev_out = s->uplo == 'L';
+    k_rhs_solve<true, T, double><<<s->ntasks2, 32, 0, st>>>(A, nk);
+    SPK_CUDA(cudaGetLastError());
+    s->launches++;
+    return SPK_OK;
 }
 
 int ensure_work(spk_system *s, size_t bytes) {
@@ -1226,7 +1582,7 @@ int ensure_residual(spk_system *s) {
     SPK_CUDA(cudaStreamSynchronize(s->stream));
     SPK_CUDA(cudaMemcpy(&h, an.p, sizeof(h), cudaMemcpyDeviceToHost));
     memcpy(&s->anorm, &h, sizeof(double));
-    SPK_TRY(s->d_norms.alloc(3 * 16));
+    SPK_TRY(s->d_norms.alloc(3 * 32));
     return SPK_OK;
 }
 
@@ -1244,7 +1600,8 @@ void residual_k(spk_system *s, int K, const double *X, long long ldx, const doub
         case 2: launch_residual<2>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 4: launch_residual<4>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 8: launch_residual<8>(s, X, ldx, B, ldb, R, ldr, st); break;
-        default: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
+        case 16: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
+        default: launch_residual<32>(s, X, ldx, B, ldb, R, ldr, st); break;
     }
 }
 
@@ -1254,7 +1611,7 @@ int scaled_residual(spk_system *s, int K, const double *R, long long ldr, const 
     SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
     k_norms<<<dim3(64, K), 256, 0, st>>>(s->n, K, R, ldr, X, ldx, B, ldb, s->d_norms.p);
     SPK_CUDA(cudaGetLastError());
-    unsigned long long h[48];
+    unsigned long long h[96];
     SPK_CUDA(cudaMemcpyAsync(h, s->d_norms.p, sizeof(unsigned long long) * 3 * K, cudaMemcpyDeviceToHost, st));
     SPK_CUDA(cudaStreamSynchronize(st));
     double worst = 0.0;
@@ -1363,7 +1720,8 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
 }
 
 // Batched solve of nrhs right-hand sides (device, column-major).  mode 0: FP64
-// tile solves in groups of up to 16.  mode 1: FP32 tile solves with FP64
+// solves in groups of 32 (right-hand-side-parallel solver) and 16/8/4/2/1 (tile
+// solver).  mode 1: FP32 tile solves with FP64
 // residuals R = B - A X and FP64 correction updates X += solve32(R), iterated
 // until the scaled residual is <= tol (tol < 0: exactly maxit corrections, no
 // host synchronisation).
@@ -1392,20 +1750,23 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     if (mode == 1) {
         SPK_TRY(ensure_fp32(s));
         SPK_TRY(ensure_residual(s));
-        if (s->rbuf.n < (size_t)(16 * n)) SPK_TRY(s->rbuf.alloc(16 * n));
-        if (s->dbuf.n < (size_t)(16 * n)) SPK_TRY(s->dbuf.alloc(16 * n));
+        if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
+        if (s->dbuf.n < (size_t)(32 * n)) SPK_TRY(s->dbuf.alloc(32 * n));
     } else if (resid) {
         SPK_TRY(ensure_residual(s));
-        if (s->rbuf.n < (size_t)(16 * n)) SPK_TRY(s->rbuf.alloc(16 * n));
+        if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
     }
     for (int g = 0; g < nrhs;) {
         const int left = nrhs - g;
-        const int K = left >= 16 ? 16 : left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+        const int K = left >= 32 ? 32 : left >= 16 ? 16 : left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
         const double *Bg = B + g * ldb;
         double *Xg = X + g * ldx;
         if (mode == 0) {
             SPK_TRY(ensure_work(s, sizeof(double) * K * n));
-            SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
+            if (K == 32)
+                SPK_TRY(launch_rhs<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
+            else
+                SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
             if (resid) {
                 residual_k(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st);
                 double r = 0;
@@ -1415,7 +1776,11 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
         } else {
             SPK_TRY(ensure_work(s, sizeof(float) * K * n));
             float *wk = (float *)s->work.p;
-            SPK_TRY(launch_tiles_k<float>(s, K, Bg, ldb, Xg, ldx, wk, st));
+            auto solve32 = [&](const double *rhs, long long ld, double *xo, long long ldo) {
+                return K == 32 ? launch_rhs<float>(s, K, rhs, ld, xo, ldo, wk, st)
+                               : launch_tiles_k<float>(s, K, rhs, ld, xo, ldo, wk, st);
+            };
+            SPK_TRY(solve32(Bg, ldb, Xg, ldx));
             int it = 0;
             double r = -1.0;
             for (;; it++) {
@@ -1427,7 +1792,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                     if ((tol >= 0 && r <= tol) || it == maxit) break;
                 }
                 if (it == maxit) break;
-                SPK_TRY(launch_tiles_k<float>(s, K, s->rbuf.p, n, s->dbuf.p, n, wk, st));
+                SPK_TRY(solve32(s->rbuf.p, n, s->dbuf.p, n));
                 k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, s->dbuf.p, Xg, ldx);
                 SPK_CUDA(cudaGetLastError());
             }

@@ -16,7 +16,7 @@ def _dev(a):
 
 
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("nrhs", [1, 3, 13, 32])
+@pytest.mark.parametrize("nrhs", [1, 3, 13, 32, 48, 70])
 def test_batch_fp64_matches_single_solves(uplo, nrhs):
     L = synth.banded_lower(60000, seed=11)
     A = L if uplo == "L" else synth.transpose(L)
@@ -33,7 +33,7 @@ def test_batch_fp64_matches_single_solves(uplo, nrhs):
 
 
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("nrhs", [1, 5, 16])
+@pytest.mark.parametrize("nrhs", [1, 5, 16, 32, 40])
 def test_batch_fp32_refinement_reaches_fp64_accuracy(uplo, nrhs):
     L = synth.banded_lower(60000, seed=12)
     A = L if uplo == "L" else synth.transpose(L)
@@ -57,6 +57,23 @@ def test_batch_fp32_fixed_iterations_and_poisson():
     it, r = S.solve_batch(dB, dX, mode=1, tol=-1.0, maxit=3)
     assert it == 3 and r <= 1e-12
     assert max(rel_err(dX.cpu().numpy()[k], Xt[k]) for k in range(4)) <= 1e-12
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("nparts", [4, 64])
+def test_batch32_wide_couplings_match_single_solves(mode, nparts):
+    """Groups of 32 on the 2-D Poisson factor (couplings 128 rows apart, beyond
+    the shared window; truncated spikes at 4 partitions)."""
+    L = synth.poisson2d_lower(128)
+    Xt, B = synth.make_rhs(L, seed=3, nrhs=33)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, nparts, "L", 1)
+    dB, dX = _dev(B), _dev(np.zeros_like(B))
+    it, r = S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8)
+    X = dX.cpu().numpy()
+    assert r <= 1e-12
+    for k in range(33):
+        assert rel_err(X[k], S.solve(B[k])) <= (1e-13 if mode == 0 else 1e-11)
+        assert rel_err(X[k], Xt[k]) <= 1e-11
 
 
 def test_batch_rejects_host_arrays_and_bad_leading_dimension():
