@@ -159,6 +159,27 @@ enum { SPK_MODE_FP64 = 0, SPK_MODE_FP32_IR = 1 };
 int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
                     double tol, int maxit, void *stream, int *iters, double *resid);
 
+/* Batched FP64 solve that allocates no device memory; no counterpart in the
+ * reference.  For callers that must not allocate once they are serving: a
+ * process whose HBM is already committed under a fixed budget (where a new
+ * cudaMalloc can fail), or a latency-critical loop where cudaMalloc/cudaFree
+ * would synchronize the device and stall work on other streams.
+ * spk_solve_batch grows a per-system work buffer on first use and whenever a
+ * larger batch arrives; this call instead uses one fixed 4 MiB scratch array
+ * (524,288 FP64 values) compiled into the library, one per device.  The
+ * right-hand sides are solved in groups of at most 524,288 / n columns;
+ * systems of more than 524,288 rows are rejected with SPK_ERR_TOO_LARGE.
+ * The first call on each device looks the scratch up (cudaGetSymbolAddress,
+ * which may load the library's device code there): make that first call, on
+ * every device you use, before any stream capture begins.  All calls on a
+ * device share the scratch, so calls whose work overlaps on the GPU (other
+ * streams, threads or systems) race and give wrong results: serialize them.
+ * Nothing in the scratch has to start at zero.  FP64 only (SPK_MODE_FP64, no
+ * residual), device arrays only, systems on the sliced-ELL layout only
+ * (spk_debug_scalar(s, "ell") == 1; others get SPK_ERR_ARG). */
+int spk_solve_batch_noalloc(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
+                            void *stream);
+
 /* Wait for the system's work and report a device-side failure (a bounded wait
  * in a kernel that gave up) as SPK_ERR_TIMEOUT. */
 int spk_check(spk_system *s);

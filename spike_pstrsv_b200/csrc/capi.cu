@@ -388,6 +388,19 @@ int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, dou
     return solve_batch(s, nrhs, B, ldb, X, ldx, mode, tol, maxit, (cudaStream_t)stream, iters, resid);
 }
 
+int spk_solve_batch_noalloc(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
+                            void *stream) {
+    if (!s || !B || !X) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!is_device_pointer(B) || !is_device_pointer(X)) {
+        set_error(SPK_ERR_ARG, "spk_solve_batch_noalloc takes device arrays");
+        return SPK_ERR_ARG;
+    }
+    return solve_batch_static(s, nrhs, B, ldb, X, ldx, (cudaStream_t)stream);
+}
+
 int spk_set_profiling(spk_system *s, int on) {
     if (!s) {
         set_error(SPK_ERR_ARG, "null argument");

@@ -33,6 +33,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <mutex>
 
 #include "spk_internal.cuh"
 
@@ -1803,6 +1804,88 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     }
     if (iters) *iters = max_it;
     if (resid) *resid = worst;
+    return SPK_OK;
+}
+
+// ---- allocation-free batched solve -------------------------------------------------
+//
+// The phase-1 work columns live in a fixed array compiled into the library
+// instead of the per-system buffer that solve_batch grows on demand, so a call
+// allocates nothing.  Groups shrink to fit (K * n <= kStaticScratch).  Every
+// work entry a solve reads is written earlier in the same solve (phase 1 rows
+// and the reduced rows), so nothing in the scratch has to start at zero.  One
+// scratch per device: solves whose work overlaps on the GPU race on it.
+
+constexpr long long kStaticScratch = 1ll << 19;  // FP64 values (4 MiB)
+static __device__ __align__(256) double g_static_scratch[kStaticScratch];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double *g_static_ptr[kMaxDevices];
+
+// Device address of the scratch on the current device, looked up once per
+// device (the lookup may load the library's device code on that device).
+int static_scratch(double **out) {
+    int dev = 0;
+    SPK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error(SPK_ERR_ARG, "device %d is beyond the %d devices the static scratch table covers", dev,
+                  kMaxDevices);
+        return SPK_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error(SPK_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                      cudaGetErrorString(e));
+            return SPK_ERR_CUDA;
+        }
+        g_static_ptr[dev] = (double *)p;
+    }
+    *out = g_static_ptr[dev];
+    return SPK_OK;
+}
+}  // namespace
+
+int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
+                       cudaStream_t st) {
+    if (!s->built) {
+        set_error(SPK_ERR_STATE, "no preprocessed system");
+        return SPK_ERR_STATE;
+    }
+    const long long n = s->n;
+    if (nrhs <= 0 || ldb < n || ldx < n) {
+        set_error(SPK_ERR_ARG, "invalid batch arguments (nrhs=%d, ldb=%lld, ldx=%lld)", nrhs, ldb, ldx);
+        return SPK_ERR_ARG;
+    }
+    if (!s->ell_ok) {
+        set_error(SPK_ERR_ARG, "the allocation-free solve needs the sliced-ELL layout (this system uses the CSR "
+                               "solver)");
+        return SPK_ERR_ARG;
+    }
+    if (n > kStaticScratch) {
+        set_error(SPK_ERR_TOO_LARGE,
+                  "system of %lld rows exceeds the allocation-free solve's static scratch of %lld FP64 values",
+                  n, kStaticScratch);
+        return SPK_ERR_TOO_LARGE;
+    }
+    double *work = nullptr;
+    SPK_TRY(static_scratch(&work));
+    for (int g = 0; g < nrhs;) {
+        const int left = nrhs - g;
+        int K = 32;
+        while (K > 1 && (K > left || K * n > kStaticScratch)) K >>= 1;
+        const double *Bg = B + g * ldb;
+        double *Xg = X + g * ldx;
+        if (K == 32)
+            SPK_TRY(launch_rhs<double>(s, K, Bg, ldb, Xg, ldx, work, st));
+        else
+            SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, work, st));
+        g += K;
+    }
     return SPK_OK;
 }
 

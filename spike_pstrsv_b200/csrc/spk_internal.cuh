@@ -163,6 +163,8 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
 int solve(spk_system *s, const double *b, double *x, cudaStream_t stream, double *phase_seconds);
 int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
                 double tol, int maxit, cudaStream_t stream, int *iters, double *resid);
+int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
+                       cudaStream_t st);
 int solve_prepare(spk_system *s);
 int check_device_error(spk_system *s);
 int collect_phase_times(spk_system *s);
