@@ -52,6 +52,53 @@ def alg_bytes(m: int, nnz: int) -> int:
     return 12 * nnz + 4 * (m + 1) + 16 * m
 
 
+def batched_bytes(m: int, nnz: int, k: int, mode: int, iters: int) -> int:
+    """Algorithmic bytes of one batch of k right-hand sides: FP64 solve
+    12 nnz + 4 (m+1) + 16 k m; FP32 solve 8 nnz + 4 (m+1) + 16 k m, plus per
+    refinement step an FP64 residual (12 nnz + 4 (m+1) + 24 k m) and an FP32
+    correction solve."""
+    if mode == 0:
+        return 12 * nnz + 4 * (m + 1) + 16 * k * m
+    solve32 = 8 * nnz + 4 * (m + 1) + 16 * k * m
+    resid = 12 * nnz + 4 * (m + 1) + 24 * k * m
+    return solve32 + iters * (resid + solve32)
+
+
+def run_batched(S, L, x_true_k, dev, stream, k: int, mode: int, steps: int, warmup: int):
+    """Batches of k right-hand sides through spk_solve_batch (FP64, or FP32 +
+    FP64 refinement with the step count a checked run needs for scaled residual
+    <= 1e-12), device-timed with CUDA events over `steps` batches."""
+    import torch
+    from spike_pstrsv_b200 import synth
+    m, nnz = L.m, L.nnz
+    Xt, Bk = synth.make_rhs(L, seed=1, nrhs=k)
+    dB = torch.from_numpy(Bk).to(dev)
+    dX = torch.zeros_like(dB)
+    sp = stream.cuda_stream
+    iters, _ = S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8, stream=sp)
+    for _ in range(warmup):
+        S.solve_batch(dB, dX, mode=mode, tol=-1.0, maxit=iters, stream=sp, want_resid=False)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = S.scalar("launches")
+    e0.record(stream)
+    for _ in range(steps):
+        S.solve_batch(dB, dX, mode=mode, tol=-1.0, maxit=iters, stream=sp, want_resid=False)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = S.scalar("launches") - l0
+    ms = e0.elapsed_time(e1) / steps
+    _, resid = S.solve_batch(dB, dX, mode=mode, tol=-1.0, maxit=iters, stream=sp)
+    X = dX.cpu().numpy()
+    err = max(float(np.linalg.norm(X[i] - Xt[i]) / np.linalg.norm(Xt[i])) for i in range(k))
+    nb = batched_bytes(m, nnz, k, mode, iters)
+    return {"mode": "fp64" if mode == 0 else "fp32_ir", "rhs_per_batch": k, "refinement_steps": iters,
+            "ms_per_batch": ms, "solves_per_s": k * 1e3 / ms, "hbm_gbs": nb / (ms * 1e-3) / 1e9,
+            "algorithmic_bytes_per_batch": nb, "scaled_residual": resid, "rel_err_vs_x_true": err,
+            "gpu_launches_per_batch": launches / steps}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -307,6 +354,12 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world / float(te.item())
+
+    # batched forms of the same system (32 right-hand sides per batch)
+    nb_steps = max(10, args.steps // 8)
+    batched = [run_batched(S, L, None, dev, stream, 32, mode, nb_steps, 3) for mode in (0, 1)]
+    for bt in batched:
+        bt["vs_plain_fp64"] = bt["solves_per_s"] / value * world
     clk = clocks.stop()
 
     x = dx.cpu().numpy()
@@ -338,6 +391,7 @@ def run_ours(args):
                "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * m,
                        "d2h_bytes_per_step": 8 * m, "api": "spike_pstrsv_solve (C ABI), pinned host b/x"},
                "gpu_launches": int(launches),
+               "batched": batched,
                "clocks": clk,
                "accuracy": {"scaled_residual": res, "rel_err_vs_x_true": err_true,
                             "e2e_vs_device_rel_diff": err_e2e}}

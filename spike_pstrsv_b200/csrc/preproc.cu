@@ -536,6 +536,12 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         return SPK_ERR_ARG;
     }
     s->built = 0;
+    // values derived from the previous matrix for the batched solves
+    s->ell_valf.release();
+    s->rdiagf.release();
+    s->diag.release();
+    s->anorm = 0.0;
+    s->ell_reach = -1;
     PhaseClock clk(ph, st);
 
     // ---- input: upload (host pointers) and mirror ('L')

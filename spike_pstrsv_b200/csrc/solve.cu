@@ -409,6 +409,7 @@ struct TileArgs {
     void *xout;           // TO
     long long ldx;
     int rev_out;
+    int acc;              // right-hand-side-parallel phase 3+4: xout += x (needs couplings within the window)
     int *err;
 };
 
@@ -698,6 +699,7 @@ struct RhsSmem {
     alignas(128) T rdn[32];
     alignas(16) int rc[33][kRhsCap];  // current tile, row l at l + 1: window offsets (fast) or columns (-1: padding)
     alignas(16) T rv[33][kRhsCap];
+    T rv0[33];  // fast tiles: coefficient of column row + 1 (taken out of rc/rv), row l at l + 1
     T rd[32];
     T win[kRhsWin + 1][kRhsLd];
     alignas(8) unsigned long long bar;
@@ -715,14 +717,17 @@ __device__ __forceinline__ void stage_rhs_tile(const TileArgs &A, RhsSmem<T> &S,
     }
 }
 
-// Right-hand sides of tile rows [a0, a1) (lane = row), zero elsewhere.
-template <typename T>
-__device__ __forceinline__ void load_rhs_tile(const TileArgs &A, int row0, int a0, int a1, int nk, T (&nb)[32]) {
-    const int row = row0 + (threadIdx.x & 31);
-    const bool ok = row >= a0 && row < a1;
+// Right-hand sides of tile row row0 + lane for the rows in [a0, a1) (other
+// lanes load row a0 and their values go unused; columns k >= nk repeat column
+// nk - 1).  Unconditional and kept as loaded (FP64), so that the loads stay in
+// flight until the next tile consumes them.
+__device__ __forceinline__ void load_rhs_tile(const TileArgs &A, int row0, int a0, int a1, int nk, double (&nb)[32]) {
+    int row = row0 + (threadIdx.x & 31);
+    if (row < a0 || row >= a1) row = a0;
     const long long o = A.rev_in ? A.n - 1 - row : row;
+    const double *src = A.rhs + o;
 #pragma unroll
-    for (int k = 0; k < 32; k++) nb[k] = (ok && k < nk) ? (T)A.rhs[k * A.ldb + o] : T(0);
+    for (int k = 0; k < 32; k++) nb[k] = src[min(k, nk - 1) * A.ldb];
 }
 
 // x of column c > r for lane's right-hand side: window below wlim, the task's
@@ -765,33 +770,61 @@ __device__ __forceinline__ void rhs_row_slots(const RhsSmem<T> &S, int lp1, int 
     }
 }
 
-// Rows a1-1 .. a0 of a tile whose slots are window offsets (branch-free).
+// One row of a fast tile in registers: slot offsets and values, the window
+// values they point at, b (the row's own window slot), the coefficient of the
+// column row + 1 and 1/diagonal.
 template <int W, typename T>
-__device__ __forceinline__ void rhs_rows_fast(RhsSmem<T> &S, int row0, int a0, int a1) {
-    const int lane = threadIdx.x & 31;
-    T *wf = &S.win[0][0];
+struct RhsRow {
     int ci[W];
     T cv[W];
-    rhs_row_slots<W, T>(S, a1 - row0, ci, cv);
-    for (int r = a1 - 1; r >= a0; r--) {
-        const int l = r - row0;
-        T xv[W];
+    T xv[W];
+    T b, v0, rd;
+};
+
+// Issue the loads of row r (tile row l).  The window loads run before x of row
+// r + 1 is stored: that column is the separate v0 term, every other column is
+// at least r + 2 and already in the window.
+template <int W, typename T>
+__device__ __forceinline__ void rhs_fetch(const RhsSmem<T> &S, int l, int r, RhsRow<W, T> &R) {
+    const int lane = threadIdx.x & 31;
+    const T *wf = &S.win[0][0];
+    rhs_row_slots<W, T>(S, l + 1, R.ci, R.cv);
 #pragma unroll
-        for (int i = 0; i < W; i++) xv[i] = wf[ci[i] + lane];
-        T *wr = wf + (r & (kRhsWin - 1)) * kRhsLd + lane;
-        T p[4] = {*wr, T(0), T(0), T(0)};
-        int ni[W];
-        T nv[W];
-        rhs_row_slots<W, T>(S, l, ni, nv);  // row l - 1 (stored at l); row -1 is the spare row 0
+    for (int i = 0; i < W; i++) R.xv[i] = wf[R.ci[i] + lane];
+    R.b = wf[(r & (kRhsWin - 1)) * kRhsLd + lane];
+    R.v0 = S.rv0[l + 1];
+    R.rd = S.rd[l & 31];
+}
+
+// x_r from the fetched row and x_{r+1} (register); stores it in the window.
+template <int W, typename T>
+__device__ __forceinline__ T rhs_finish(RhsSmem<T> &S, int r, const RhsRow<W, T> &R, T xnext) {
+    const int lane = threadIdx.x & 31;
+    T p[4] = {R.b, T(0), T(0), T(0)};
 #pragma unroll
-        for (int i = 0; i < W; i++) p[i & 3] = fma(-cv[i], xv[i], p[i & 3]);
-        *wr = ((p[0] + p[1]) + (p[2] + p[3])) * S.rd[l];
-#pragma unroll
-        for (int i = 0; i < W; i++) {
-            ci[i] = ni[i];
-            cv[i] = nv[i];
-        }
+    for (int i = 0; i < W; i++) p[i & 3] = fma(-R.cv[i], R.xv[i], p[i & 3]);
+    const T x = (((p[1] + p[2]) + p[3]) + fma(-R.v0, xnext, p[0])) * R.rd;
+    S.win[r & (kRhsWin - 1)][lane] = x;
+    return x;
+}
+
+// Rows a1-1 .. a0 of a tile whose slots are window offsets (branch-free),
+// software-pipelined one row ahead; two rows per trip so the register sets
+// alternate instead of being copied.
+template <int W, typename T>
+__device__ __forceinline__ void rhs_rows_fast(RhsSmem<T> &S, int row0, int a0, int a1, int wlim) {
+    const int lane = threadIdx.x & 31;
+    T xnext = a1 < wlim ? S.win[a1 & (kRhsWin - 1)][lane] : T(0);
+    RhsRow<W, T> A, B;
+    rhs_fetch<W, T>(S, a1 - 1 - row0, a1 - 1, A);
+    int r = a1 - 1;
+    for (; r - 1 >= a0; r -= 2) {
+        rhs_fetch<W, T>(S, r - 1 - row0, r - 1, B);
+        xnext = rhs_finish<W, T>(S, r, A, xnext);
+        rhs_fetch<W, T>(S, r - 2 - row0, r - 2, A);  // row a0 - 1 at most: the spare row 0 / zero slots
+        xnext = rhs_finish<W, T>(S, r - 1, B, xnext);
     }
+    if (r >= a0) rhs_finish<W, T>(S, r, A, xnext);
 }
 
 // Rows a1-1 .. a0 of any tile: columns (slots >= kRhsCap from global memory),
@@ -820,7 +853,8 @@ __device__ void rhs_rows_general(const TileArgs &A, RhsSmem<T> &S, int row0, int
 }
 
 template <bool FULL, typename T, typename TO>
-__device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int lo, int hi, int hi_ext, int nk) {
+__device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int lo, int hi, int hi_ext, int halo_end,
+                          int nk) {
     const int lane = threadIdx.x & 31;
     if (hi <= lo) return true;
     const bool act = lane < nk;
@@ -832,8 +866,8 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
     int p_next = ntiles > 1 ? A.ell_ptr[jt - 1] : 0;
     __syncwarp();
     if (lane == 0) stage_rhs_tile<T>(A, S, jt, p_lo, p_hi);
-    T nb[32];
-    load_rhs_tile<T>(A, 32 * jt, max(lo, 32 * jt), hi, nk, nb);
+    double nb[32];
+    load_rhs_tile(A, 32 * jt, max(lo, 32 * jt), hi, nk, nb);
     for (int it = 0; it < ntiles; it++) {
         const int j = jt - it;
         const int row0 = 32 * j;
@@ -843,7 +877,7 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
         if (mine) {
             T *w = S.win[row & (kRhsWin - 1)];
 #pragma unroll
-            for (int k = 0; k < 32; k++) w[k] = nb[k];
+            for (int k = 0; k < 32; k++) w[k] = (T)nb[k];
         }
         {
             const long long t0 = clock64();
@@ -858,7 +892,7 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
         // transpose the staged tile to row-major (lane = row)
         const int width = (p_hi - p_lo) >> 5;
         const int nst = min(width, kRhsCap);
-        const int wlim = min(row0 + kRhsWin, hi_ext);
+        const int wlim = min(row0 + kRhsWin, FULL ? halo_end : hi_ext);
         int cl[kRhsCap];
         T vl[kRhsCap];
         bool local = true;
@@ -866,10 +900,21 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
         for (int q = 0; q < kRhsCap; q++) {
             cl[q] = q < nst ? S.c[q * 32 + lane] : -1;
             vl[q] = q < nst ? S.v[q * 32 + lane] : T(0);
-            if (cl[q] == row) cl[q] = -1;
+            if (cl[q] == row || (!FULL && cl[q] >= hi_ext)) cl[q] = -1;  // padding; phase 1: no coupling
             if (mine && cl[q] >= wlim) local = false;
         }
         const bool fast = __all_sync(0xffffffffu, local) && width <= kRhsCap;
+        T v0 = T(0);
+        if (fast) {
+#pragma unroll
+            for (int q = 0; q < kRhsCap; q++)
+                if (cl[q] == row + 1) {
+                    v0 = vl[q];
+                    cl[q] = -1;
+                    vl[q] = T(0);
+                }
+        }
+        S.rv0[lane + 1] = v0;
 #pragma unroll
         for (int q = 0; q < kRhsCap; q += 4) {
             int4 o;
@@ -896,12 +941,18 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
         if (it + 1 < ntiles) {
             if (lane == 0) stage_rhs_tile<T>(A, S, j - 1, p_next, p_lo);
             if (it + 2 < ntiles) p_next2 = A.ell_ptr[j - 2];
-            load_rhs_tile<T>(A, row0 - 32, max(lo, row0 - 32), row0, nk, nb);
+            load_rhs_tile(A, row0 - 32, max(lo, row0 - 32), row0, nk, nb);
+        }
+        double xold[32];  // acc: the tile's current output, loaded while the rows are solved
+        if (FULL && A.acc) {
+            const long long o = A.rev_out ? n - 1 - (mine ? row : a0) : (mine ? row : a0);
+#pragma unroll
+            for (int k = 0; k < 32; k++) xold[k] = ((const double *)A.xout)[min(k, nk - 1) * A.ldx + o];
         }
         if (fast) {
-            if (width <= 4) rhs_rows_fast<4, T>(S, row0, a0, a1);
-            else if (width <= 8) rhs_rows_fast<8, T>(S, row0, a0, a1);
-            else rhs_rows_fast<16, T>(S, row0, a0, a1);
+            if (width <= 4) rhs_rows_fast<4, T>(S, row0, a0, a1, wlim);
+            else if (width <= 8) rhs_rows_fast<8, T>(S, row0, a0, a1, wlim);
+            else rhs_rows_fast<16, T>(S, row0, a0, a1, wlim);
         } else {
             rhs_rows_general<FULL, T, TO>(A, S, row0, a0, a1, width, p_lo, wlim, hi_ext, act);
         }
@@ -911,7 +962,7 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
             const T *w = S.win[row & (kRhsWin - 1)];
 #pragma unroll
             for (int k = 0; k < 32; k++)
-                if (k < nk) xout[k * A.ldx + o] = (TO)w[k];
+                if (k < nk) xout[k * A.ldx + o] = (FULL && A.acc) ? (TO)(xold[k] + (double)w[k]) : (TO)w[k];
         }
         __syncwarp();
         p_hi = p_lo;
@@ -919,6 +970,27 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
         p_next = p_next2;
     }
     return true;
+}
+
+// Phase-1 values of rows [lo, hi) (the rows above a task, which its couplings
+// read) into the window.
+template <typename T>
+__device__ void rhs_load_halo(const TileArgs &A, RhsSmem<T> &S, int lo, int hi, int nk) {
+    const int lane = threadIdx.x & 31;
+    const T *xfix = (const T *)A.xfix;
+    for (int r0 = lo; r0 < hi; r0 += 32) {
+        const int r = r0 + lane;
+        const bool ok = r < hi;
+        T v[32];
+#pragma unroll
+        for (int k = 0; k < 32; k++) v[k] = (ok && k < nk) ? xfix[(long long)k * A.n + r] : T(0);
+        if (ok) {
+            T *w = S.win[r & (kRhsWin - 1)];
+#pragma unroll
+            for (int k = 0; k < 32; k++) w[k] = v[k];
+        }
+    }
+    __syncwarp();
 }
 
 // Copy rows [lo, hi) of the phase-1 values into the output and the window, 32
@@ -932,13 +1004,18 @@ __device__ void rhs_copy_rows(const TileArgs &A, RhsSmem<T> &S, int lo, int hi, 
         const int r = r0 + lane;
         const bool ok = r < hi;
         T v[32];
+        double old[32];
+        const long long o = A.rev_out ? A.n - 1 - (ok ? r : lo) : (ok ? r : lo);
 #pragma unroll
         for (int k = 0; k < 32; k++) v[k] = (ok && k < nk) ? xfix[(long long)k * A.n + r] : T(0);
+        if (A.acc) {
+#pragma unroll
+            for (int k = 0; k < 32; k++) old[k] = ((const double *)A.xout)[min(k, nk - 1) * A.ldx + o];
+        }
         if (ok) {
-            const long long o = A.rev_out ? A.n - 1 - r : r;
 #pragma unroll
             for (int k = 0; k < 32; k++)
-                if (k < nk) xout[k * A.ldx + o] = (TO)v[k];
+                if (k < nk) xout[k * A.ldx + o] = A.acc ? (TO)(old[k] + (double)v[k]) : (TO)v[k];
             if (r < lo + kRhsWin) {
                 T *w = S.win[r & (kRhsWin - 1)];
 #pragma unroll
@@ -963,16 +1040,20 @@ __global__ void __launch_bounds__(32) k_rhs_solve(TileArgs A, int nk) {
 #pragma unroll
     for (int q = 0; q < kRhsCap; q += 4) *reinterpret_cast<int4 *>(&S.rc[0][q]) = make_int4(0, 0, 0, 0);
     if (lane < kRhsCap) S.rv[0][lane] = T(0);
+    if (lane == 0) S.rv0[0] = T(0);
     __syncwarp();
     unsigned phase = 0u;
     const SegTask t = A.tasks[task];
+    // phase 3+4: the rows above the task (3 tiles) come from the phase-1 values
+    const int halo_end = FULL ? min(A.n, t.hi + kRhsWin - 32) : t.hi;
+    if (FULL) rhs_load_halo<T>(A, S, t.hi, halo_end, nk);
     if (FULL && t.tail > t.hi) rhs_copy_rows<T, TO>(A, S, t.hi, t.tail, nk);
     if (t.skip_hi > t.skip_lo) {
-        if (!rhs_range<FULL, T, TO>(A, S, phase, t.skip_hi, t.hi, t.hi, nk)) return;
+        if (!rhs_range<FULL, T, TO>(A, S, phase, t.skip_hi, t.hi, t.hi, halo_end, nk)) return;
         rhs_copy_rows<T, TO>(A, S, t.skip_lo, t.skip_hi, nk);
-        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.skip_lo, t.hi, nk);
+        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.skip_lo, t.hi, halo_end, nk);
     } else {
-        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.hi, t.hi, nk);
+        rhs_range<FULL, T, TO>(A, S, phase, t.lo, t.hi, t.hi, halo_end, nk);
     }
 }
 
@@ -1111,6 +1192,198 @@ __global__ void k_residual(int n, const int *__restrict__ ptr, const double *__r
     }
 #pragma unroll
     for (int k = 0; k < K; k++) R[k * ldr + orow] = B[k * ldb + orow] - acc[k];
+}
+
+// R = B - A X for up to 32 right-hand sides with lane = right-hand side
+// (FP64).  A block of kResWarps warps walks a chunk of kResChunk tiles
+// top-down (U order).  Each tile's X rows enter a 128-row shared window
+// ([row mod 128][lane]; it holds the tile and the 96 rows above, which its
+// couplings read), its B rows a 32 x 33 tile that turns into R, its slots a
+// slot-major copy; thread (warp w, lane l) moves rows row0 + l of columns
+// 8w .. 8w+7 (coalesced along rows) and the next tile's values are loaded into
+// registers while the current tile is computed.  The warps split the tile's
+// rows.  Columns beyond the window (couplings wider than 96 rows) and slots
+// beyond kResCap read global memory.  With norms != nullptr it also folds
+// max |R|, max |X|, max |B| per right-hand side into norms[3k..3k+2] (as
+// k_norms).
+constexpr int kResWarps = 4;
+constexpr int kResChunk = 32;  // tiles per block
+constexpr int kResCap = 16;    // staged slots per row
+constexpr int kResCols = 32 / kResWarps;
+
+struct ResSmem {
+    double win[kRhsWin][33];
+    double bt[32][33];
+    double v[kResCap * 32];
+    int c[kResCap * 32];
+    double dg[32];
+    unsigned long long nrm[kResWarps][3][32];
+};
+
+struct ResTile {
+    double x[kResCols], b[kResCols];
+    double v[kResCap * 32 / (32 * kResWarps)];
+    int c[kResCap * 32 / (32 * kResWarps)];
+    double dg;
+};
+
+__global__ void __launch_bounds__(32 * kResWarps)
+k_rhs_residual(int n, int nk, const int *__restrict__ ptr, const double *__restrict__ ev, const int *__restrict__ ec,
+               const double *__restrict__ diag, const double *__restrict__ X, long long ldx,
+               const double *__restrict__ B, long long ldb, double *__restrict__ R, long long ldr, int rev,
+               unsigned long long *__restrict__ norms) {
+    extern __shared__ __align__(16) unsigned char res_raw[];
+    ResSmem &S = *reinterpret_cast<ResSmem *>(res_raw);
+    constexpr int NT = 32 * kResWarps, NS = kResCap * 32 / NT;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ntiles = (n + 31) >> 5;
+    const int jb = blockIdx.x * kResChunk, je = min(ntiles, jb + kResChunk);  // tiles [jb, je)
+    if (jb >= je) return;
+    const int k0 = warp * kResCols;
+    auto orow = [&](int r) -> long long { return rev ? (long long)n - 1 - r : r; };
+    // halo: X rows [hi, hi + 96) above the chunk
+    {
+        const int hi = min(n, 32 * je), he = min(n, hi + kRhsWin - 32);
+        for (int r = hi + lane; r < he; r += 32)
+#pragma unroll
+            for (int u = 0; u < kResCols; u++)
+                if (k0 + u < nk) S.win[r & (kRhsWin - 1)][k0 + u] = X[(k0 + u) * ldx + orow(r)];
+    }
+    auto fetch = [&](int j, ResTile &T) {
+        const int r = min(32 * j + lane, n - 1);
+        const long long o = orow(r);
+#pragma unroll
+        for (int u = 0; u < kResCols; u++) {
+            const int k = min(k0 + u, nk - 1);
+            T.x[u] = X[k * ldx + o];
+            T.b[u] = B[k * ldb + o];
+        }
+        const int p0 = ptr[j], ne = min(ptr[j + 1] - p0, kResCap * 32);
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+            const int e = tid + NT * i;
+            T.v[i] = e < ne ? ev[p0 + e] : 0.0;
+            T.c[i] = e < ne ? ec[p0 + e] : 0;
+        }
+        T.dg = diag[min(32 * j + lane, n - 1)];
+    };
+    ResTile cur;
+    fetch(je - 1, cur);
+    double mr = 0, mx = 0, mb = 0;
+    for (int j = je - 1; j >= jb; j--) {
+        const int row0 = 32 * j, rows = min(32, n - row0);
+        // current tile into shared memory
+        if (lane < rows) {
+            double *w = S.win[(row0 + lane) & (kRhsWin - 1)];
+#pragma unroll
+            for (int u = 0; u < kResCols; u++) {
+                w[k0 + u] = cur.x[u];
+                S.bt[lane][k0 + u] = cur.b[u];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NS; i++) {
+            S.v[tid + NT * i] = cur.v[i];
+            S.c[tid + NT * i] = cur.c[i];
+        }
+        if (warp == 0) S.dg[lane] = cur.dg;
+        const int p0 = ptr[j], width = (ptr[j + 1] - p0) >> 5, nst = min(width, kResCap);
+        bool local = width <= kResCap;
+#pragma unroll
+        for (int i = 0; i < NS; i++) local = local && cur.c[i] < row0 + kRhsWin;
+        local = __syncthreads_and(local);
+        if (j > jb) fetch(j - 1, cur);
+        if (local) {
+            // every column inside the window: branch-free slot loop
+            const double *wf = &S.win[0][0] + lane;
+            for (int l = warp; l < rows; l += kResWarps) {
+                const int r = row0 + l;
+                double a[4] = {0.0, 0.0, 0.0, 0.0};
+                int q = 0;
+                for (; q + 4 <= width; q += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int c = S.c[(q + u) * 32 + l];
+                        a[u] = fma(S.v[(q + u) * 32 + l], wf[(c & (kRhsWin - 1)) * 33], a[u]);
+                    }
+                }
+                for (; q < width; q++) {
+                    const int c = S.c[q * 32 + l];
+                    a[0] = fma(S.v[q * 32 + l], wf[(c & (kRhsWin - 1)) * 33], a[0]);
+                }
+                const double xr = wf[(r & (kRhsWin - 1)) * 33];
+                const double b = S.bt[l][lane];
+                const double res = b - fma(S.dg[l], xr, (a[0] + a[1]) + (a[2] + a[3]));
+                S.bt[l][lane] = res;
+                mr = fmax(mr, fabs(res));
+                mx = fmax(mx, fabs(xr));
+                mb = fmax(mb, fabs(b));
+            }
+        } else
+        for (int l = warp; l < rows; l += kResWarps) {
+            const int r = row0 + l;
+            double a0 = 0.0, a1 = 0.0;
+            int q = 0;
+            for (; q + 2 <= nst; q += 2) {
+                const int c0 = S.c[q * 32 + l], c1 = S.c[(q + 1) * 32 + l];
+                const double v0 = S.v[q * 32 + l], v1 = S.v[(q + 1) * 32 + l];
+                const double x0 = c0 < row0 + kRhsWin ? S.win[c0 & (kRhsWin - 1)][lane]
+                                                      : (lane < nk ? X[lane * ldx + orow(c0)] : 0.0);
+                const double x1 = c1 < row0 + kRhsWin ? S.win[c1 & (kRhsWin - 1)][lane]
+                                                      : (lane < nk ? X[lane * ldx + orow(c1)] : 0.0);
+                a0 = fma(v0, x0, a0);
+                a1 = fma(v1, x1, a1);
+            }
+            for (; q < width; q++) {
+                const int c = q < nst ? S.c[q * 32 + l] : ec[p0 + 32 * q + l];
+                const double v = q < nst ? S.v[q * 32 + l] : ev[p0 + 32 * q + l];
+                const double x = c < row0 + kRhsWin ? S.win[c & (kRhsWin - 1)][lane]
+                                                    : (lane < nk ? X[lane * ldx + orow(c)] : 0.0);
+                a0 = fma(v, x, a0);
+            }
+            const double xr = S.win[r & (kRhsWin - 1)][lane];
+            const double b = S.bt[l][lane];
+            const double res = b - fma(S.dg[l], xr, a0 + a1);
+            S.bt[l][lane] = res;
+            mr = fmax(mr, fabs(res));
+            mx = fmax(mx, fabs(xr));
+            mb = fmax(mb, fabs(b));
+        }
+        __syncthreads();
+        if (lane < rows) {
+            const long long o = orow(row0 + lane);
+#pragma unroll
+            for (int u = 0; u < kResCols; u++)
+                if (k0 + u < nk) R[(k0 + u) * ldr + o] = S.bt[lane][k0 + u];
+        }
+        __syncthreads();  // before the next tile rewrites bt, the slots and the window
+    }
+    if (norms) {
+        S.nrm[warp][0][lane] = __double_as_longlong(mr);
+        S.nrm[warp][1][lane] = __double_as_longlong(mx);
+        S.nrm[warp][2][lane] = __double_as_longlong(mb);
+        __syncthreads();
+        if (warp == 0 && lane < nk) {
+#pragma unroll
+            for (int w = 0; w < 3; w++) {
+                unsigned long long m = 0;
+#pragma unroll
+                for (int u = 0; u < kResWarps; u++) m = max(m, S.nrm[u][w][lane]);
+                atomicMax(&norms[3 * lane + w], m);
+            }
+        }
+    }
+}
+
+// Largest distance from a tile's first row to a column of its slots.
+__global__ void k_ell_reach(int ntiles, const int *__restrict__ ptr, const int *__restrict__ col, int *__restrict__ out) {
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= ntiles) return;
+    int m = 0;
+    for (int e = ptr[j] + (threadIdx.x & 31); e < ptr[j + 1]; e += 32) m = max(m, col[e] - 32 * j);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // Per right-hand side: max |R|, max |X|, max |B| (bit patterns of non-negative
@@ -1514,7 +1787,7 @@ int launch_tiles_k(spk_system *s, int K, const double *rhs, long long ldb, doubl
 // solver; work holds 32 columns (leading dimension n).
 template <typename T>
 int launch_rhs(spk_system *s, int nk, const double *rhs, long long ldb, double *xo, long long ldx, T *work,
-               cudaStream_t st) {
+               cudaStream_t st, bool acc = false) {
     TileArgs A{};
     A.ell_val = sizeof(T) == 8 ? (const void *)s->ell_val.p : (const void *)s->ell_valf.p;
     A.ell_col = s->ell_col.p;
@@ -1546,9 +1819,26 @@ int launch_rhs(spk_system *s, int nk, const double *rhs, long long ldb, double *
     A.xout = xo;
     A.ldx = ldx;
     A.rev_out = s->uplo == 'L';
+    A.acc = acc;
     k_rhs_solve<true, T, double><<<s->ntasks2, 32, 0, st>>>(A, nk);
     SPK_CUDA(cudaGetLastError());
     s->launches++;
+    return SPK_OK;
+}
+
+// Coupling reach of the ELL copy (computed once).
+int ensure_reach(spk_system *s) {
+    if (s->ell_reach >= 0) return SPK_OK;
+    DBuf<int> d;
+    SPK_TRY(d.alloc(1));
+    SPK_CUDA(cudaMemsetAsync(d.p, 0, sizeof(int), s->stream));
+    const int ntiles = (s->n + 31) >> 5;
+    k_ell_reach<<<(ntiles + 7) / 8, 256, 0, s->stream>>>(ntiles, s->ell_ptr.p, s->ell_col.p, d.p);
+    SPK_CUDA(cudaGetLastError());
+    int h = 0;
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    SPK_CUDA(cudaMemcpy(&h, d.p, sizeof(int), cudaMemcpyDeviceToHost));
+    s->ell_reach = h;
     return SPK_OK;
 }
 
@@ -1594,24 +1884,40 @@ void launch_residual(spk_system *s, const double *X, long long ldx, const double
                                                      B, ldb, R, ldr, s->uplo == 'L');
 }
 
-void residual_k(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
-                long long ldr, cudaStream_t st) {
+// R = B - A X (FP64) for K right-hand sides; with norms, also the per-column
+// max |R|, |X|, |B| in d_norms (read back by scaled_residual).
+int residual(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
+             long long ldr, cudaStream_t st, bool norms) {
+    if (norms) SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
+    if (K == 32) {
+        SPK_CUDA(cudaFuncSetAttribute(k_rhs_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(ResSmem)));
+        const int ntiles = (s->n + 31) >> 5;
+        const int blocks = (ntiles + kResChunk - 1) / kResChunk;
+        k_rhs_residual<<<blocks, 32 * kResWarps, sizeof(ResSmem), st>>>(
+            s->n, K, s->ell_ptr.p, s->ell_val.p, s->ell_col.p, s->diag.p, X, ldx, B, ldb, R, ldr, s->uplo == 'L',
+            norms ? s->d_norms.p : nullptr);
+        SPK_CUDA(cudaGetLastError());
+        return SPK_OK;
+    }
     switch (K) {
         case 1: launch_residual<1>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 2: launch_residual<2>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 4: launch_residual<4>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 8: launch_residual<8>(s, X, ldx, B, ldb, R, ldr, st); break;
-        case 16: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
-        default: launch_residual<32>(s, X, ldx, B, ldb, R, ldr, st); break;
+        default: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
     }
+    SPK_CUDA(cudaGetLastError());
+    if (norms) {
+        k_norms<<<dim3(64, K), 256, 0, st>>>(s->n, K, R, ldr, X, ldx, B, ldb, s->d_norms.p);
+        SPK_CUDA(cudaGetLastError());
+    }
+    return SPK_OK;
 }
 
-// max over the K right-hand sides of ||R||_inf / (||A||_inf ||X||_inf + ||B||_inf)
-int scaled_residual(spk_system *s, int K, const double *R, long long ldr, const double *X, long long ldx,
-                    const double *B, long long ldb, cudaStream_t st, double *out) {
-    SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
-    k_norms<<<dim3(64, K), 256, 0, st>>>(s->n, K, R, ldr, X, ldx, B, ldb, s->d_norms.p);
-    SPK_CUDA(cudaGetLastError());
+// max over the K right-hand sides of ||R||_inf / (||A||_inf ||X||_inf + ||B||_inf),
+// from the norms residual() left in d_norms
+int scaled_residual(spk_system *s, int K, cudaStream_t st, double *out) {
     unsigned long long h[96];
     SPK_CUDA(cudaMemcpyAsync(h, s->d_norms.p, sizeof(unsigned long long) * 3 * K, cudaMemcpyDeviceToHost, st));
     SPK_CUDA(cudaStreamSynchronize(st));
@@ -1751,6 +2057,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     if (mode == 1) {
         SPK_TRY(ensure_fp32(s));
         SPK_TRY(ensure_residual(s));
+        SPK_TRY(ensure_reach(s));
         if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
         if (s->dbuf.n < (size_t)(32 * n)) SPK_TRY(s->dbuf.alloc(32 * n));
     } else if (resid) {
@@ -1769,9 +2076,9 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
             else
                 SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
             if (resid) {
-                residual_k(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st);
+                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st, true));
                 double r = 0;
-                SPK_TRY(scaled_residual(s, K, s->rbuf.p, n, Xg, ldx, Bg, ldb, st, &r));
+                SPK_TRY(scaled_residual(s, K, st, &r));
                 worst = std::max(worst, r);
             }
         } else {
@@ -1787,15 +2094,20 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
             for (;; it++) {
                 const bool check = tol >= 0 || (resid && it == maxit);
                 if (tol < 0 && it == maxit && !resid) break;
-                residual_k(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st);
+                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st, check));
                 if (check) {
-                    SPK_TRY(scaled_residual(s, K, s->rbuf.p, n, Xg, ldx, Bg, ldb, st, &r));
+                    SPK_TRY(scaled_residual(s, K, st, &r));
                     if ((tol >= 0 && r <= tol) || it == maxit) break;
                 }
                 if (it == maxit) break;
-                SPK_TRY(solve32(s->rbuf.p, n, s->dbuf.p, n));
-                k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, s->dbuf.p, Xg, ldx);
-                SPK_CUDA(cudaGetLastError());
+                if (K == 32 && s->ell_reach < kRhsWin) {
+                    // correction added in place by phase 3+4 (no coupling leaves the window)
+                    SPK_TRY(launch_rhs<float>(s, K, s->rbuf.p, n, Xg, ldx, wk, st, true));
+                } else {
+                    SPK_TRY(solve32(s->rbuf.p, n, s->dbuf.p, n));
+                    k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, s->dbuf.p, Xg, ldx);
+                    SPK_CUDA(cudaGetLastError());
+                }
             }
             max_it = std::max(max_it, it);
             if (r >= 0) worst = std::max(worst, r);

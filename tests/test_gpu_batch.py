@@ -86,3 +86,18 @@ def test_batch_rejects_host_arrays_and_bad_leading_dimension():
     dB = torch.zeros((2, L.m - 1), dtype=torch.float64, device="cuda:0")
     with pytest.raises(spk.SpkError):
         S.solve_batch(dB, dB.clone(), mode=0)
+
+
+def test_batch_fp32_after_repreprocessing_the_same_handle():
+    """Mixed-precision state (FP32 copies, FP64 diagonal) follows a new matrix
+    preprocessed on the same handle."""
+    S = spk.System()
+    for seed in (31, 32):
+        L = synth.banded_lower(40000, seed=seed)
+        Xt, B = synth.make_rhs(L, seed=seed, nrhs=32)
+        S.preproc(L.a, L.ia, L.ja, L.m, 16, "L", 1)
+        dB, dX = _dev(B), _dev(np.zeros_like(B))
+        it, r = S.solve_batch(dB, dX, mode=1, tol=1e-12, maxit=8)
+        assert r <= 1e-12
+        X = dX.cpu().numpy()
+        assert max(rel_err(X[k], Xt[k]) for k in range(32)) <= 1e-12
