@@ -207,6 +207,34 @@ int spk_debug_array(const spk_system *s, const char *name, void *dst, long long 
                     long long *count, char *type);
 long long spk_debug_scalar(const spk_system *s, const char *name);
 
+/* Serving loop (no reference counterpart; the reference has one global system
+ * and no request handling).  The server keeps preprocessed systems resident in
+ * HBM under hbm_budget_bytes (footprint admission; idle systems are destroyed in
+ * least-recently-used order when a matrix must be admitted) and serves solve
+ * requests with nslots worker threads, each with its own CUDA stream: a free
+ * worker packs up to 32 queued right-hand sides of the matrix whose oldest
+ * request waited longest into one spk_solve_batch, so requests that arrive
+ * while other batches run join the next batch and batches of different
+ * matrices overlap on the device.  Requests take host arrays (column-major,
+ * leading dimension n) that must stay valid until spk_server_wait returns.
+ * SPK_MODE_FP32_IR requests iterate to scaled residual <= 1e-12. */
+typedef struct spk_server spk_server;
+int spk_server_create(spk_server **out, long long hbm_budget_bytes, int nslots);
+int spk_server_destroy(spk_server *srv);
+/* Register (or replace, when idle) matrix `id`; the server keeps a host copy of
+ * the CSR arrays and preprocesses it when a batch first needs it. */
+int spk_server_put_matrix(spk_server *srv, int id, const double *a, const int *ia, const int *ja, int n,
+                          int nparts, char uplo);
+int spk_server_submit(spk_server *srv, int id, int nrhs, const double *b, double *x, int mode, long long *ticket);
+/* Block until the request is done: latency (submit to result in x, seconds), the
+ * batch's scaled residual (FP32_IR; -1 otherwise), refinement steps and the
+ * batch's right-hand-side count. */
+int spk_server_wait(spk_server *srv, long long ticket, double *latency_s, double *resid, int *iters,
+                    int *batch_rhs);
+/* out[0..8]: resident bytes, staging bytes, resident systems, evictions,
+ * preprocessings, batches, right-hand sides batched, requests completed, budget. */
+int spk_server_stats(spk_server *srv, long long *out, int count);
+
 /* The system used by the Part-1 entry points (NULL before the first preproc). */
 spk_system *spk_legacy_system(void);
 

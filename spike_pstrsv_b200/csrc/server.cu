@@ -1,0 +1,441 @@
+// Serving loop: resident preprocessed systems, footprint admission with LRU
+// eviction, and continuous batching of solve requests.
+//
+// The reference splits preprocessing (spike_pstrsv_preproc, src/spike_pstrsv.c:40-81)
+// from solving (spike_pstrsv_solve, :149-239) but keeps a single global system.
+// The server keeps many systems (spk_system handles) resident in HBM and serves
+// solve requests against them:
+//
+// * Matrices are registered with spk_server_put_matrix (the server keeps a host
+//   copy of the CSR arrays).  A matrix is preprocessed when a batch first needs
+//   it; its device footprint (spk_debug_scalar "device_bytes", which grows when
+//   the batched solves add their work buffers) counts against the HBM budget.
+//   When admitting a matrix would exceed the budget, idle resident systems are
+//   destroyed in least-recently-used order; a matrix that still does not fit
+//   waits until running batches release theirs.
+// * Requests (nrhs right-hand sides in host memory) queue per matrix.  Each of
+//   nslots worker threads owns a CUDA stream and device/pinned staging buffers;
+//   a free worker takes the matrix whose oldest request waited longest, packs up
+//   to kBatchRhs right-hand sides of that matrix's queued requests into one
+//   batch (requests that arrive while other batches run join the next batch of
+//   their matrix), and runs copy-in, spk_solve_batch and copy-out on its
+//   stream, so batches of different matrices overlap on the device.  One matrix
+//   is in at most one batch at a time (its handle's work buffers are shared).
+// * Each request records its latency (submit to result in host memory) and the
+//   scaled residual of its batch.
+
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "spk_internal.cuh"
+
+namespace {
+
+constexpr int kBatchRhs = 32;
+
+double wall_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Request {
+    long long ticket = 0;
+    int id = 0, nrhs = 0, mode = 0;
+    const double *b = nullptr;
+    double *x = nullptr;
+    double t_submit = 0, t_start = 0, t_done = 0, resid = -1;
+    int status = SPK_OK, iters = 0, batch_rhs = 0;
+    bool done = false;
+};
+
+struct Matrix {
+    int id = 0, n = 0, nparts = 0;
+    char uplo = 'L';
+    std::vector<double> a;
+    std::vector<int> ia, ja;
+    spk_system *sys = nullptr;
+    long long bytes = 0;      // device footprint while resident
+    long long last_use = 0;   // LRU clock
+    bool busy = false;        // in a batch (or being preprocessed)
+    std::deque<Request *> pending;
+};
+
+struct Slot {
+    cudaStream_t st = nullptr;
+    double *dB = nullptr, *dX = nullptr, *hB = nullptr, *hX = nullptr;
+    size_t cap = 0;  // doubles in each buffer
+    std::thread th;
+};
+
+}  // namespace
+
+struct spk_server {
+    long long budget = 0;
+    long long resident = 0;     // sum of resident systems' footprints
+    long long workspace = 0;    // staging buffers of the slots
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::map<int, Matrix *> mats;
+    std::unordered_map<long long, Request *> reqs;
+    std::vector<Slot *> slots;
+    long long next_ticket = 1, clock = 0;
+    long long evictions = 0, preprocs = 0, batches = 0, batched_rhs = 0, completed = 0;
+    int device = 0;
+    bool stop = false;
+};
+
+namespace {
+
+using spk::set_error;
+
+// Host copy of a matrix registration.
+int copy_csr(Matrix *M, const double *a, const int *ia, const int *ja, int n) {
+    if (n <= 0 || !a || !ia || !ja) {
+        set_error(SPK_ERR_ARG, "invalid matrix (n=%d)", n);
+        return SPK_ERR_ARG;
+    }
+    const int nnz = ia[n];
+    if (ia[0] != 0 || nnz <= 0) {
+        set_error(SPK_ERR_INPUT, "ia must start at 0 and end at nnz > 0");
+        return SPK_ERR_INPUT;
+    }
+    M->n = n;
+    M->a.assign(a, a + nnz);
+    M->ia.assign(ia, ia + n + 1);
+    M->ja.assign(ja, ja + nnz);
+    return SPK_OK;
+}
+
+// Device footprint estimate before preprocessing: the CSR copy, the ELL copy,
+// the spike/reduced pools and one batch of work buffers scale with nnz and n.
+long long estimate_bytes(const Matrix *M) {
+    const long long nnz = (long long)M->a.size(), n = M->n;
+    return 40 * nnz + 64 * n + (long long)kBatchRhs * 8 * 3 * n;
+}
+
+// Destroy idle resident systems, least recently used first, until `need` more
+// bytes fit.  Called with the lock held; returns whether they fit.
+bool make_room(spk_server *S, long long need, const Matrix *keep) {
+    while (S->resident + S->workspace + need > S->budget) {
+        Matrix *victim = nullptr;
+        for (auto &kv : S->mats) {
+            Matrix *M = kv.second;
+            if (M == keep || !M->sys || M->busy) continue;
+            if (!victim || M->last_use < victim->last_use) victim = M;
+        }
+        if (!victim) return false;
+        spk_destroy(victim->sys);
+        victim->sys = nullptr;
+        S->resident -= victim->bytes;
+        victim->bytes = 0;
+        S->evictions++;
+    }
+    return true;
+}
+
+int ensure_slot_capacity(spk_server *S, Slot *sl, size_t doubles) {
+    if (sl->cap >= doubles) return SPK_OK;
+    if (sl->dB) cudaFree(sl->dB);
+    if (sl->dX) cudaFree(sl->dX);
+    if (sl->hB) cudaFreeHost(sl->hB);
+    if (sl->hX) cudaFreeHost(sl->hX);
+    sl->dB = sl->dX = sl->hB = sl->hX = nullptr;
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        S->workspace -= (long long)(2 * sizeof(double) * sl->cap);
+    }
+    sl->cap = 0;
+    SPK_CUDA(cudaMalloc((void **)&sl->dB, doubles * sizeof(double)));
+    SPK_CUDA(cudaMalloc((void **)&sl->dX, doubles * sizeof(double)));
+    SPK_CUDA(cudaHostAlloc((void **)&sl->hB, doubles * sizeof(double), cudaHostAllocDefault));
+    SPK_CUDA(cudaHostAlloc((void **)&sl->hX, doubles * sizeof(double), cudaHostAllocDefault));
+    sl->cap = doubles;
+    std::lock_guard<std::mutex> g(S->mu);
+    S->workspace += (long long)(2 * sizeof(double) * doubles);
+    return SPK_OK;
+}
+
+// Copy-in, batched solve and copy-out of one batch on the slot's stream.
+int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch, int mode, int *iters,
+              double *resid) {
+    const long long n = M->n;
+    int k = 0;
+    for (Request *r : batch) k += r->nrhs;
+    SPK_TRY(ensure_slot_capacity(S, sl, (size_t)k * n));
+    int c = 0;
+    for (Request *r : batch) {
+        memcpy(sl->hB + (size_t)c * n, r->b, sizeof(double) * r->nrhs * n);
+        c += r->nrhs;
+    }
+    SPK_CUDA(cudaMemcpyAsync(sl->dB, sl->hB, sizeof(double) * k * n, cudaMemcpyHostToDevice, sl->st));
+    // FP32 + refinement iterates to scaled residual <= 1e-12 (and reports it);
+    // FP64 batches skip the residual pass
+    SPK_TRY(spk_solve_batch(M->sys, k, sl->dB, n, sl->dX, n, mode, mode == SPK_MODE_FP32_IR ? 1e-12 : -1.0, 10,
+                            (void *)sl->st, iters, mode == SPK_MODE_FP32_IR ? resid : nullptr));
+    SPK_CUDA(cudaMemcpyAsync(sl->hX, sl->dX, sizeof(double) * k * n, cudaMemcpyDeviceToHost, sl->st));
+    SPK_CUDA(cudaStreamSynchronize(sl->st));
+    SPK_TRY(spk_check(M->sys));
+    c = 0;
+    for (Request *r : batch) {
+        memcpy(r->x, sl->hX + (size_t)c * n, sizeof(double) * r->nrhs * n);
+        c += r->nrhs;
+    }
+    return SPK_OK;
+}
+
+// The matrix whose oldest queued request is the oldest among idle matrices.
+Matrix *pick(spk_server *S) {
+    Matrix *best = nullptr;
+    for (auto &kv : S->mats) {
+        Matrix *M = kv.second;
+        if (M->busy || M->pending.empty()) continue;
+        if (!best || M->pending.front()->t_submit < best->pending.front()->t_submit) best = M;
+    }
+    return best;
+}
+
+void worker(spk_server *S, Slot *sl) {
+    cudaSetDevice(S->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        Matrix *M = nullptr;
+        S->cv_work.wait(lk, [&] { return S->stop || (M = pick(S)) != nullptr; });
+        if (S->stop) return;
+        // batch: queued requests of one mode, up to kBatchRhs right-hand sides (at least one request)
+        std::vector<Request *> batch;
+        const int mode = M->pending.front()->mode;
+        int k = 0;
+        for (auto it = M->pending.begin(); it != M->pending.end();) {
+            Request *r = *it;
+            if (r->mode != mode || (!batch.empty() && k + r->nrhs > kBatchRhs)) {
+                ++it;
+                continue;
+            }
+            batch.push_back(r);
+            k += r->nrhs;
+            it = M->pending.erase(it);
+            if (k >= kBatchRhs) break;
+        }
+        M->busy = true;
+        int status = SPK_OK;
+        if (!M->sys) {
+            // admission by footprint, LRU eviction of idle systems
+            const long long need = estimate_bytes(M);
+            while (!make_room(S, need, M)) {
+                bool others_busy = false;
+                for (auto &kv : S->mats)
+                    if (kv.second != M && kv.second->busy) others_busy = true;
+                if (!others_busy) break;  // nothing will be released: run over budget
+                S->cv_done.wait(lk);
+            }
+            lk.unlock();
+            spk_system *sys = nullptr;
+            status = spk_create(&sys);
+            if (status == SPK_OK)
+                status = spk_preproc(sys, M->a.data(), M->ia.data(), M->ja.data(), M->n, M->nparts, M->uplo, 1,
+                                     nullptr, nullptr);
+            lk.lock();
+            if (status == SPK_OK) {
+                M->sys = sys;
+                M->bytes = spk_debug_scalar(sys, "device_bytes");
+                S->resident += M->bytes;
+                S->preprocs++;
+            } else if (sys) {
+                spk_destroy(sys);
+            }
+        }
+        int iters = 0;
+        double resid = -1;
+        const double t0 = wall_s();
+        for (Request *r : batch) r->t_start = t0;
+        if (status == SPK_OK) {
+            lk.unlock();
+            status = run_batch(S, sl, M, batch, mode, &iters, &resid);
+            lk.lock();
+            // the batched solves may have grown the system's work buffers
+            const long long now = spk_debug_scalar(M->sys, "device_bytes");
+            S->resident += now - M->bytes;
+            M->bytes = now;
+        }
+        const double t1 = wall_s();
+        for (Request *r : batch) {
+            r->t_done = t1;
+            r->status = status;
+            r->resid = resid;
+            r->iters = iters;
+            r->batch_rhs = k;
+            r->done = true;
+        }
+        M->busy = false;
+        M->last_use = ++S->clock;
+        S->batches++;
+        S->batched_rhs += k;
+        S->completed += (long long)batch.size();
+        make_room(S, 0, nullptr);  // back under budget where growth pushed it over
+        S->cv_done.notify_all();
+        S->cv_work.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int spk_server_create(spk_server **out, long long hbm_budget_bytes, int nslots) {
+    if (!out || hbm_budget_bytes <= 0 || nslots <= 0 || nslots > 64) {
+        set_error(SPK_ERR_ARG, "invalid server arguments (budget=%lld, slots=%d)", hbm_budget_bytes, nslots);
+        return SPK_ERR_ARG;
+    }
+    spk_server *S = new spk_server();
+    S->budget = hbm_budget_bytes;
+    cudaGetDevice(&S->device);
+    for (int i = 0; i < nslots; i++) {
+        Slot *sl = new Slot();
+        if (cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete sl;
+            set_error(SPK_ERR_CUDA, "cudaStreamCreate failed");
+            spk_server_destroy(S);
+            return SPK_ERR_CUDA;
+        }
+        S->slots.push_back(sl);
+    }
+    for (Slot *sl : S->slots) sl->th = std::thread(worker, S, sl);
+    *out = S;
+    return SPK_OK;
+}
+
+int spk_server_destroy(spk_server *S) {
+    if (!S) return SPK_OK;
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    for (Slot *sl : S->slots)
+        if (sl->th.joinable()) sl->th.join();
+    for (Slot *sl : S->slots) {
+        if (sl->dB) cudaFree(sl->dB);
+        if (sl->dX) cudaFree(sl->dX);
+        if (sl->hB) cudaFreeHost(sl->hB);
+        if (sl->hX) cudaFreeHost(sl->hX);
+        if (sl->st) cudaStreamDestroy(sl->st);
+        delete sl;
+    }
+    for (auto &kv : S->mats) {
+        if (kv.second->sys) spk_destroy(kv.second->sys);
+        delete kv.second;
+    }
+    for (auto &kv : S->reqs) delete kv.second;
+    delete S;
+    return SPK_OK;
+}
+
+int spk_server_put_matrix(spk_server *S, int id, const double *a, const int *ia, const int *ja, int n, int nparts,
+                          char uplo) {
+    if (!S || nparts <= 0 || nparts > n || (uplo != 'L' && uplo != 'U' && uplo != 'l' && uplo != 'u')) {
+        set_error(SPK_ERR_ARG, "invalid matrix registration (n=%d, nparts=%d, uplo=%c)", n, nparts, uplo);
+        return SPK_ERR_ARG;
+    }
+    Matrix *M = new Matrix();
+    M->id = id;
+    M->nparts = nparts;
+    M->uplo = (uplo == 'l' || uplo == 'L') ? 'L' : 'U';
+    const int rc = copy_csr(M, a, ia, ja, n);
+    if (rc != SPK_OK) {
+        delete M;
+        return rc;
+    }
+    std::lock_guard<std::mutex> g(S->mu);
+    auto it = S->mats.find(id);
+    if (it != S->mats.end()) {
+        Matrix *old = it->second;
+        if (old->busy || !old->pending.empty()) {
+            delete M;
+            set_error(SPK_ERR_STATE, "matrix %d has requests in flight", id);
+            return SPK_ERR_STATE;
+        }
+        if (old->sys) {
+            spk_destroy(old->sys);
+            S->resident -= old->bytes;
+        }
+        delete old;
+    }
+    S->mats[id] = M;
+    return SPK_OK;
+}
+
+int spk_server_submit(spk_server *S, int id, int nrhs, const double *b, double *x, int mode, long long *ticket) {
+    if (!S || !b || !x || !ticket || nrhs <= 0 || (mode != SPK_MODE_FP64 && mode != SPK_MODE_FP32_IR)) {
+        set_error(SPK_ERR_ARG, "invalid request (nrhs=%d, mode=%d)", nrhs, mode);
+        return SPK_ERR_ARG;
+    }
+    Request *r = new Request();
+    r->id = id;
+    r->nrhs = nrhs;
+    r->mode = mode;
+    r->b = b;
+    r->x = x;
+    r->t_submit = wall_s();
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        auto it = S->mats.find(id);
+        if (it == S->mats.end()) {
+            delete r;
+            set_error(SPK_ERR_ARG, "unknown matrix %d", id);
+            return SPK_ERR_ARG;
+        }
+        r->ticket = S->next_ticket++;
+        S->reqs[r->ticket] = r;
+        it->second->pending.push_back(r);
+        *ticket = r->ticket;
+    }
+    S->cv_work.notify_one();
+    return SPK_OK;
+}
+
+int spk_server_wait(spk_server *S, long long ticket, double *latency_s, double *resid, int *iters,
+                    int *batch_rhs) {
+    if (!S) {
+        set_error(SPK_ERR_ARG, "null server");
+        return SPK_ERR_ARG;
+    }
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end()) {
+        set_error(SPK_ERR_ARG, "unknown ticket %lld", ticket);
+        return SPK_ERR_ARG;
+    }
+    Request *r = it->second;
+    S->cv_done.wait(lk, [&] { return r->done; });
+    if (latency_s) *latency_s = r->t_done - r->t_submit;
+    if (resid) *resid = r->resid;
+    if (iters) *iters = r->iters;
+    if (batch_rhs) *batch_rhs = r->batch_rhs;
+    const int status = r->status;
+    S->reqs.erase(it);
+    delete r;
+    if (status != SPK_OK) set_error(status, "request %lld failed (status %d)", ticket, status);
+    return status;
+}
+
+int spk_server_stats(spk_server *S, long long *out, int count) {
+    if (!S || !out) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> g(S->mu);
+    long long nres = 0;
+    for (auto &kv : S->mats) nres += kv.second->sys != nullptr;
+    const long long v[9] = {S->resident, S->workspace, nres, S->evictions, S->preprocs,
+                            S->batches, S->batched_rhs, S->completed, S->budget};
+    for (int i = 0; i < count && i < 9; i++) out[i] = v[i];
+    return SPK_OK;
+}
+
+}  // extern "C"
