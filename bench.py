@@ -360,6 +360,12 @@ def run_ours(args):
     batched = [run_batched(S, L, None, dev, stream, 32, mode, nb_steps, 3) for mode in (0, 1)]
     for bt in batched:
         bt["vs_plain_fp64"] = bt["solves_per_s"] / value * world
+    # served form: Poisson-arrival request stream through the serving loop
+    # (reduced pool; python -m spike_pstrsv_b200.serve_bench --full runs the full one)
+    served = None
+    if world == 1 and not args.no_served:
+        from spike_pstrsv_b200 import serve_bench
+        served = serve_bench.run(full=False, rates=(50.0, 500.0), nreq=300)
     clk = clocks.stop()
 
     x = dx.cpu().numpy()
@@ -392,6 +398,7 @@ def run_ours(args):
                        "d2h_bytes_per_step": 8 * m, "api": "spike_pstrsv_solve (C ABI), pinned host b/x"},
                "gpu_launches": int(launches),
                "batched": batched,
+               "served": served,
                "clocks": clk,
                "accuracy": {"scaled_residual": res, "rel_err_vs_x_true": err_true,
                             "e2e_vs_device_rel_diff": err_e2e}}
@@ -411,6 +418,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--P", type=int, default=1024, help="nthreads = Spike partitions")
+    ap.add_argument("--no-served", action="store_true", help="skip the serving-loop stream")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

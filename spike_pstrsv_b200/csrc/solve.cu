@@ -1889,7 +1889,7 @@ void launch_residual(spk_system *s, const double *X, long long ldx, const double
 int residual(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
              long long ldr, cudaStream_t st, bool norms) {
     if (norms) SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
-    if (K == 32) {
+    if (K > 16) {
         SPK_CUDA(cudaFuncSetAttribute(k_rhs_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(ResSmem)));
         const int ntiles = (s->n + 31) >> 5;
@@ -2064,14 +2064,26 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
         SPK_TRY(ensure_residual(s));
         if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
     }
+    // The right-hand-side-parallel solver runs one warp per task along the task's
+    // rows; it pays off once the tasks fill the GPU (two per SM).  With fewer
+    // tasks the tile solver (rows of a tile across the lanes) has the shorter path.
+    int dev = 0, sms = 148;
+    SPK_CUDA(cudaGetDevice(&dev));
+    SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const bool wide_ok = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms;
     for (int g = 0; g < nrhs;) {
         const int left = nrhs - g;
-        const int K = left >= 32 ? 32 : left >= 16 ? 16 : left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+        // 17..32 columns: one right-hand-side-parallel pass (work holds 32 columns);
+        // fewer (or few tasks): the tile solver in power-of-two groups
+        const int K = (wide_ok && left > 16) ? std::min(left, 32)
+                                             : left >= 16 ? 16 : left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
+        const bool rhs_path = K > 16;
+        const long long wcols = rhs_path ? 32 : K;
         const double *Bg = B + g * ldb;
         double *Xg = X + g * ldx;
         if (mode == 0) {
-            SPK_TRY(ensure_work(s, sizeof(double) * K * n));
-            if (K == 32)
+            SPK_TRY(ensure_work(s, sizeof(double) * wcols * n));
+            if (rhs_path)
                 SPK_TRY(launch_rhs<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
             else
                 SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
@@ -2082,10 +2094,10 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                 worst = std::max(worst, r);
             }
         } else {
-            SPK_TRY(ensure_work(s, sizeof(float) * K * n));
+            SPK_TRY(ensure_work(s, sizeof(float) * wcols * n));
             float *wk = (float *)s->work.p;
             auto solve32 = [&](const double *rhs, long long ld, double *xo, long long ldo) {
-                return K == 32 ? launch_rhs<float>(s, K, rhs, ld, xo, ldo, wk, st)
+                return rhs_path ? launch_rhs<float>(s, K, rhs, ld, xo, ldo, wk, st)
                                : launch_tiles_k<float>(s, K, rhs, ld, xo, ldo, wk, st);
             };
             SPK_TRY(solve32(Bg, ldb, Xg, ldx));
@@ -2100,7 +2112,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                     if ((tol >= 0 && r <= tol) || it == maxit) break;
                 }
                 if (it == maxit) break;
-                if (K == 32 && s->ell_reach < kRhsWin) {
+                if (rhs_path && s->ell_reach < kRhsWin) {
                     // correction added in place by phase 3+4 (no coupling leaves the window)
                     SPK_TRY(launch_rhs<float>(s, K, s->rbuf.p, n, Xg, ldx, wk, st, true));
                 } else {

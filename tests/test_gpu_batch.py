@@ -16,12 +16,13 @@ def _dev(a):
 
 
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("nrhs", [1, 3, 13, 32, 48, 70])
+@pytest.mark.parametrize("nrhs", [1, 3, 13, 20, 32, 48, 70])
 def test_batch_fp64_matches_single_solves(uplo, nrhs):
     L = synth.banded_lower(60000, seed=11)
     A = L if uplo == "L" else synth.transpose(L)
     Xt, B = synth.make_rhs(A, seed=5, nrhs=nrhs)
-    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 16, uplo, 1)
+    # 512 partitions: groups of 17..32 columns take the right-hand-side-parallel solver
+    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 16 if nrhs <= 16 else 512, uplo, 1)
     dB = _dev(B)
     dX = _dev(np.zeros_like(B))
     it, r = S.solve_batch(dB, dX, mode=0)
@@ -33,12 +34,12 @@ def test_batch_fp64_matches_single_solves(uplo, nrhs):
 
 
 @pytest.mark.parametrize("uplo", ["L", "U"])
-@pytest.mark.parametrize("nrhs", [1, 5, 16, 32, 40])
+@pytest.mark.parametrize("nrhs", [1, 5, 16, 27, 32, 40])
 def test_batch_fp32_refinement_reaches_fp64_accuracy(uplo, nrhs):
     L = synth.banded_lower(60000, seed=12)
     A = L if uplo == "L" else synth.transpose(L)
     Xt, B = synth.make_rhs(A, seed=6, nrhs=nrhs)
-    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 32, uplo, 1)
+    S = spk.System().preproc(A.a, A.ia, A.ja, A.m, 32 if nrhs <= 16 else 512, uplo, 1)
     dB = _dev(B)
     dX = _dev(np.zeros_like(B))
     it, r = S.solve_batch(dB, dX, mode=1, tol=1e-12, maxit=8)
@@ -60,18 +61,18 @@ def test_batch_fp32_fixed_iterations_and_poisson():
 
 
 @pytest.mark.parametrize("mode", [0, 1])
-@pytest.mark.parametrize("nparts", [4, 64])
+@pytest.mark.parametrize("nparts", [4, 64, 512])
 def test_batch32_wide_couplings_match_single_solves(mode, nparts):
-    """Groups of 32 on the 2-D Poisson factor (couplings 128 rows apart, beyond
+    """Groups of 32 and 25 on the 2-D Poisson factor (couplings 128 rows apart, beyond
     the shared window; truncated spikes at 4 partitions)."""
     L = synth.poisson2d_lower(128)
-    Xt, B = synth.make_rhs(L, seed=3, nrhs=33)
+    Xt, B = synth.make_rhs(L, seed=3, nrhs=57)  # groups of 32 and 25
     S = spk.System().preproc(L.a, L.ia, L.ja, L.m, nparts, "L", 1)
     dB, dX = _dev(B), _dev(np.zeros_like(B))
     it, r = S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8)
     X = dX.cpu().numpy()
     assert r <= 1e-12
-    for k in range(33):
+    for k in range(57):
         assert rel_err(X[k], S.solve(B[k])) <= (1e-13 if mode == 0 else 1e-11)
         assert rel_err(X[k], Xt[k]) <= 1e-11
 
@@ -95,9 +96,24 @@ def test_batch_fp32_after_repreprocessing_the_same_handle():
     for seed in (31, 32):
         L = synth.banded_lower(40000, seed=seed)
         Xt, B = synth.make_rhs(L, seed=seed, nrhs=32)
-        S.preproc(L.a, L.ia, L.ja, L.m, 16, "L", 1)
+        S.preproc(L.a, L.ia, L.ja, L.m, 400, "L", 1)
         dB, dX = _dev(B), _dev(np.zeros_like(B))
         it, r = S.solve_batch(dB, dX, mode=1, tol=1e-12, maxit=8)
         assert r <= 1e-12
         X = dX.cpu().numpy()
         assert max(rel_err(X[k], Xt[k]) for k in range(32)) <= 1e-12
+
+
+@pytest.mark.parametrize("nparts", [8, 512])
+def test_batch_paths_agree(nparts):
+    """Few tasks (tile solver groups) and many tasks (right-hand-side-parallel
+    groups) give the same FP64 answer."""
+    L = synth.banded_lower(50000, seed=41)
+    Xt, B = synth.make_rhs(L, seed=41, nrhs=24)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, nparts, "L", 1)
+    dB, dX = _dev(B), _dev(np.zeros_like(B))
+    S.solve_batch(dB, dX, mode=0)
+    X = dX.cpu().numpy()
+    for k in range(24):
+        assert rel_err(X[k], Xt[k]) <= 1e-12
+        assert rel_err(X[k], S.solve(B[k])) <= 1e-13
