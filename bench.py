@@ -366,6 +366,12 @@ def run_ours(args):
     if world == 1 and not args.no_served:
         from spike_pstrsv_b200 import serve_bench
         served = serve_bench.run(full=False, rates=(50.0, 500.0), nreq=300)
+    # many independent systems in one captured launch sequence (reduced pool of
+    # 128 systems; python -m spike_pstrsv_b200.group runs the 512-system form)
+    systems = None
+    if world == 1 and not args.no_served:
+        from spike_pstrsv_b200 import group
+        systems = group.run(count=128, reps=5)
     clk = clocks.stop()
 
     x = dx.cpu().numpy()
@@ -399,6 +405,7 @@ def run_ours(args):
                "gpu_launches": int(launches),
                "batched": batched,
                "served": served,
+               "batched_systems": systems,
                "clocks": clk,
                "accuracy": {"scaled_residual": res, "rel_err_vs_x_true": err_true,
                             "e2e_vs_device_rel_diff": err_e2e}}

@@ -207,6 +207,28 @@ int spk_debug_array(const spk_system *s, const char *name, void *dst, long long 
                     long long *count, char *type);
 long long spk_debug_scalar(const spk_system *s, const char *name);
 
+/* Many systems solved by one captured launch sequence (no reference
+ * counterpart).  count preprocessed systems (sliced-ELL layout), system i with
+ * nrhs[i] right-hand sides in device array B[i] (column-major, leading dimension
+ * ldb[i]) and solutions X[i] (ldx[i]).  The columns are split into width classes
+ * 16/8/4/2/1; per class one launch runs the phase-1 tasks of every system from a
+ * flat work list (longest tasks first), one the reduced solves, one phase 3+4
+ * (FP32 + refinement adds residual and update launches per step).  The sequence
+ * is captured on `stream` (not the legacy default stream) into a CUDA graph that
+ * spk_group_solve replays; the arrays must stay in place.  mode SPK_MODE_FP64 or
+ * SPK_MODE_FP32_IR with `iters` fixed refinement steps.  spk_group_residual
+ * returns the largest scaled residual over all systems and columns;
+ * spk_group_info: "kernels" (launches in the graph), "virtual_systems",
+ * "columns", "task_items", "pool_bytes". */
+typedef struct spk_group spk_group;
+int spk_group_create(spk_group **out, int count, spk_system *const *systems, const int *nrhs,
+                     const double *const *B, const long long *ldb, double *const *X, const long long *ldx, int mode,
+                     int iters, void *stream);
+int spk_group_solve(spk_group *g, void *stream);
+int spk_group_residual(spk_group *g, void *stream, double *worst);
+long long spk_group_info(const spk_group *g, const char *name);
+int spk_group_destroy(spk_group *g);
+
 /* Serving loop (no reference counterpart; the reference has one global system
  * and no request handling).  The server keeps preprocessed systems resident in
  * HBM under hbm_budget_bytes (footprint admission; idle systems are destroyed in

@@ -29,6 +29,7 @@
 // uplo='L' (x_L[i] = x_U[n-1-i]) is folded into the right-hand-side loads and
 // the solution stores.
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -641,9 +642,8 @@ __device__ void tile_copy_rows(const TileArgs &A, TileSmemK<K, T> &S, int lo, in
 }
 
 template <bool FULL, int K, typename T, typename TO>
-__global__ void __launch_bounds__(32) k_tile_solve(TileArgs A) {
+__device__ __forceinline__ void tile_task(const TileArgs &A, int task) {
     __shared__ TileSmemK<K, T> S;
-    const int task = blockIdx.x;
     if (task >= A.ntasks) return;
     const int lane = threadIdx.x;
     if (lane == 0) {
@@ -664,6 +664,20 @@ __global__ void __launch_bounds__(32) k_tile_solve(TileArgs A) {
     } else {
         tile_range<FULL, K, T, TO>(A, S, phase, t.lo, t.hi, t.hi);
     }
+}
+
+template <bool FULL, int K, typename T, typename TO>
+__global__ void __launch_bounds__(32) k_tile_solve(TileArgs A) {
+    tile_task<FULL, K, T, TO>(A, blockIdx.x);
+}
+
+// Many systems in one launch: block b solves task work[b].y of the system
+// whose arguments are args[work[b].x] (a flat work list, longest tasks first).
+template <bool FULL, int K, typename T, typename TO>
+__global__ void __launch_bounds__(32) k_tile_multi(const TileArgs *__restrict__ args, const int2 *__restrict__ work) {
+    const int2 w = work[blockIdx.x];
+    const TileArgs A = args[w.x];
+    tile_task<FULL, K, T, TO>(A, w.y);
 }
 
 // ---- right-hand-side-parallel tile solver (batches of up to 32) -----------------
@@ -1136,10 +1150,10 @@ template <int K>
 constexpr int red_threads() { return K >= 16 ? 512 : 1024; }  // K >= 16: registers for the K sums
 
 template <int K, typename T>
-__global__ void __launch_bounds__(red_threads<K>())
-k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
-                  const int *__restrict__ mapRedX, const int *__restrict__ IT, const int *__restrict__ JT,
-                  const double *__restrict__ Tv, T *__restrict__ xbuf, int n) {
+__device__ __forceinline__ void reduced_body(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
+                                             const int *__restrict__ mapRedX, const int *__restrict__ IT,
+                                             const int *__restrict__ JT, const double *__restrict__ Tv,
+                                             T *__restrict__ xbuf, int n) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int li = 0; li < nlvl; li++) {
         for (int q = lvl_off[li] + warp; q < lvl_off[li + 1]; q += nwarps) {
@@ -1167,14 +1181,38 @@ k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off,
     }
 }
 
+template <int K, typename T>
+__global__ void __launch_bounds__(red_threads<K>())
+k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
+                  const int *__restrict__ mapRedX, const int *__restrict__ IT, const int *__restrict__ JT,
+                  const double *__restrict__ Tv, T *__restrict__ xbuf, int n) {
+    reduced_body<K, T>(rows, lvl_off, nlvl, mapRedX, IT, JT, Tv, xbuf, n);
+}
+
+// Reduced solves of many systems: block b takes the system of args[list[b]].
+struct RedArgs {
+    const int *rows, *lvl_off;
+    int nlvl;
+    const int *mapRedX, *IT, *JT;
+    const double *Tv;
+    void *xbuf;  // T
+    int n;
+};
+
+template <int K, typename T>
+__global__ void __launch_bounds__(red_threads<K>()) k_reduced_multi(const RedArgs *__restrict__ args) {
+    const RedArgs A = args[blockIdx.x];
+    reduced_body<K, T>(A.rows, A.lvl_off, A.nlvl, A.mapRedX, A.IT, A.JT, A.Tv, (T *)A.xbuf, A.n);
+}
+
 // R = B - A X in FP64 on the ELL copy (plus the diagonal), in the caller's order
 // (rev: caller row i is U row n-1-i).  One thread per row; a warp covers a tile.
 template <int K>
-__global__ void k_residual(int n, const int *__restrict__ ptr, const double *__restrict__ ev,
-                           const int *__restrict__ ec, const double *__restrict__ diag,
-                           const double *__restrict__ X, long long ldx, const double *__restrict__ B,
-                           long long ldb, double *__restrict__ R, long long ldr, int rev) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void residual_row(int r, int n, const int *__restrict__ ptr, const double *__restrict__ ev,
+                                             const int *__restrict__ ec, const double *__restrict__ diag,
+                                             const double *__restrict__ X, long long ldx,
+                                             const double *__restrict__ B, long long ldb, double *__restrict__ R,
+                                             long long ldr, int rev) {
     if (r >= n) return;
     const int j = r >> 5;
     const int w = (ptr[j + 1] - ptr[j]) >> 5;
@@ -1192,6 +1230,72 @@ __global__ void k_residual(int n, const int *__restrict__ ptr, const double *__r
     }
 #pragma unroll
     for (int k = 0; k < K; k++) R[k * ldr + orow] = B[k * ldb + orow] - acc[k];
+}
+
+template <int K>
+__global__ void k_residual(int n, const int *__restrict__ ptr, const double *__restrict__ ev,
+                           const int *__restrict__ ec, const double *__restrict__ diag,
+                           const double *__restrict__ X, long long ldx, const double *__restrict__ B,
+                           long long ldb, double *__restrict__ R, long long ldr, int rev) {
+    residual_row<K>(blockIdx.x * blockDim.x + threadIdx.x, n, ptr, ev, ec, diag, X, ldx, B, ldb, R, ldr, rev);
+}
+
+// Residuals (and, with `norms`, per-column max |R|, |X|, |B|) and X += D of many
+// systems: block b covers rows 256 * work[b].y .. of the system args[work[b].x].
+struct VecArgs {
+    int n, rev;
+    const int *ptr;
+    const double *ev;
+    const int *ec;
+    const double *diag;
+    double *X;
+    long long ldx;
+    const double *B;
+    long long ldb;
+    double *R;  // residual (ld n)
+    const double *D;  // correction (ld n)
+    unsigned long long *norms;  // 3 per column
+};
+
+template <int K>
+__global__ void __launch_bounds__(256) k_residual_multi(const VecArgs *__restrict__ args, const int2 *__restrict__ work,
+                                                       int with_norms) {
+    const int2 w = work[blockIdx.x];
+    const VecArgs &A = args[w.x];
+    const int r = w.y * 256 + threadIdx.x;
+    residual_row<K>(r, A.n, A.ptr, A.ev, A.ec, A.diag, A.X, A.ldx, A.B, A.ldb, A.R, A.n, A.rev);
+    if (!with_norms) return;
+    const long long o = A.rev ? A.n - 1 - (long long)min(r, A.n - 1) : min(r, A.n - 1);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double mr = 0, mx = 0, mb = 0;
+        if (r < A.n) {
+            mr = fabs(A.R[k * (long long)A.n + o]);
+            mx = fabs(A.X[k * A.ldx + o]);
+            mb = fabs(A.B[k * A.ldb + o]);
+        }
+#pragma unroll
+        for (int s = 16; s; s >>= 1) {
+            mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, s));
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+            mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, s));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(&A.norms[3 * k + 0], __double_as_longlong(mr));
+            atomicMax(&A.norms[3 * k + 1], __double_as_longlong(mx));
+            atomicMax(&A.norms[3 * k + 2], __double_as_longlong(mb));
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) k_axpy_multi(const VecArgs *__restrict__ args, const int2 *__restrict__ work) {
+    const int2 w = work[blockIdx.x];
+    const VecArgs &A = args[w.x];
+    const int r = w.y * 256 + threadIdx.x;
+    if (r >= A.n) return;
+#pragma unroll
+    for (int k = 0; k < K; k++) A.X[k * A.ldx + r] += A.D[k * (long long)A.n + r];
 }
 
 // R = B - A X for up to 32 right-hand sides with lane = right-hand side
@@ -2255,3 +2359,419 @@ int clobber_rhs(spk_system *s, const double *x, double *b, cudaStream_t st) {
 }
 
 }  // namespace spk
+
+// ---- many systems in one captured launch sequence (spk_group) --------------------
+//
+// Every system's right-hand sides are split into width classes K in
+// {16, 8, 4, 2, 1} ("virtual systems": one system, K columns).  Per class, one
+// k_tile_multi launch runs the phase-1 tasks of all its virtual systems from a
+// flat work list (longest tasks first), one k_reduced_multi launch their
+// reduced solves (a block per virtual system), one k_tile_multi launch their
+// phase 3+4 tasks; FP32 + refinement adds k_residual_multi and k_axpy_multi
+// over flat row-block lists.  The whole sequence is captured once into a CUDA
+// graph and replayed by spk_group_solve.
+
+namespace spk {
+namespace {
+
+constexpr int kGroupK[5] = {16, 8, 4, 2, 1};
+
+struct GroupVS {
+    spk_system *s;
+    int sys;  // index in the group
+    int K, col0;
+    const double *B;
+    long long ldb;
+    double *X;
+    long long ldx;
+    char *work;
+    double *R, *D;
+};
+
+struct GroupClass {
+    int K = 0;
+    DBuf<TileArgs> a1, a4, c1, c4;  // solve and correction-solve arguments (phase 1, phase 3+4)
+    DBuf<int2> w1, w4, vw;
+    DBuf<RedArgs> red, cred;
+    DBuf<VecArgs> va;
+    int n1 = 0, n4 = 0, nred = 0, nvw = 0;
+    std::vector<int> vs;  // virtual systems of the class
+};
+
+}  // namespace
+}  // namespace spk
+
+struct spk_group {
+    int mode = 0, iters = 0;
+    std::vector<spk_system *> sys;
+    std::vector<spk::GroupVS> vs;
+    spk::GroupClass cls[5];
+    spk::DBuf<char> pool;
+    spk::DBuf<unsigned long long> norms;
+    long long norm_cols = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;
+};
+
+namespace spk {
+namespace {
+
+TileArgs make_args(const GroupVS &v, bool fp32, bool phase4, const double *rhs, long long ldb, double *xo,
+                   long long ldx) {
+    spk_system *s = v.s;
+    TileArgs A{};
+    A.ell_val = fp32 ? (const void *)s->ell_valf.p : (const void *)s->ell_val.p;
+    A.ell_col = s->ell_col.p;
+    A.ell_ptr = s->ell_ptr.p;
+    A.rdiag = fp32 ? (const void *)s->rdiagf.p : (const void *)s->rdiag.p;
+    A.n = s->n;
+    A.rhs = rhs;
+    A.ldb = ldb;
+    A.rev_in = s->uplo == 'L';
+    A.err = s->d_err.p;
+    if (!phase4) {
+        A.tasks = s->d_tasks1.p;
+        A.ntasks = s->ntasks1;
+        A.xout = v.work;
+        A.ldx = s->n;
+    } else {
+        A.tasks = s->d_tasks2.p;
+        A.ntasks = s->ntasks2;
+        A.xfix = v.work;
+        A.xout = xo;
+        A.ldx = ldx;
+        A.rev_out = s->uplo == 'L';
+    }
+    return A;
+}
+
+template <typename T>
+int upload_vec(DBuf<T> &d, const std::vector<T> &h) {
+    SPK_TRY(d.alloc(std::max<size_t>(h.size(), 1)));
+    if (!h.empty()) SPK_CUDA(cudaMemcpy(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return SPK_OK;
+}
+
+// Work lists and argument tables of one class.
+int build_class(spk_group *g, GroupClass &c, const std::vector<std::vector<SegTask>> &t1,
+                const std::vector<std::vector<SegTask>> &t4) {
+    const bool fp32 = g->mode == 1;
+    std::vector<TileArgs> a1, a4, c1, c4;
+    std::vector<RedArgs> red, cred;
+    std::vector<VecArgs> va;
+    std::vector<std::pair<long long, int2>> w1, w4;
+    std::vector<int2> vw;
+    for (size_t i = 0; i < c.vs.size(); i++) {
+        const GroupVS &v = g->vs[c.vs[i]];
+        spk_system *s = v.s;
+        a1.push_back(make_args(v, fp32, false, v.B, v.ldb, nullptr, 0));
+        a4.push_back(make_args(v, fp32, true, v.B, v.ldb, v.X, v.ldx));
+        if (fp32) {
+            c1.push_back(make_args(v, true, false, v.R, s->n, nullptr, 0));
+            c4.push_back(make_args(v, true, true, v.R, s->n, v.D, s->n));
+        }
+        if (s->redNec && s->ntasks1)
+            for (int t = 0; t < s->ntasks1; t++) {
+                const SegTask &q = t1[v.sys][t];
+                w1.push_back({(long long)(q.hi - q.lo), make_int2((int)i, t)});
+            }
+        for (int t = 0; t < s->ntasks2; t++) {
+            const SegTask &q = t4[v.sys][t];
+            w4.push_back({(long long)(q.hi - q.lo) + (q.tail - q.hi), make_int2((int)i, t)});
+        }
+        if (s->redNec && s->nkept) {
+            RedArgs r{s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p, s->IT.p, s->JT.p, s->T.p, v.work,
+                      s->n};
+            red.push_back(r);
+            cred.push_back(r);
+        }
+        VecArgs a{};
+        a.n = s->n;
+        a.rev = s->uplo == 'L';
+        a.ptr = s->ell_ptr.p;
+        a.ev = s->ell_val.p;
+        a.ec = s->ell_col.p;
+        a.diag = s->diag.p;
+        a.X = v.X;
+        a.ldx = v.ldx;
+        a.B = v.B;
+        a.ldb = v.ldb;
+        a.R = v.R;
+        a.D = v.D;
+        a.norms = g->norms.p + 3ll * (v.col0);
+        va.push_back(a);
+        for (int b = 0; b * 256 < s->n; b++) vw.push_back(make_int2((int)i, b));
+    }
+    auto sorted = [](std::vector<std::pair<long long, int2>> &w) {
+        std::stable_sort(w.begin(), w.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+        std::vector<int2> o;
+        for (auto &e : w) o.push_back(e.second);
+        return o;
+    };
+    SPK_TRY(upload_vec(c.a1, a1));
+    SPK_TRY(upload_vec(c.a4, a4));
+    if (fp32) {
+        SPK_TRY(upload_vec(c.c1, c1));
+        SPK_TRY(upload_vec(c.c4, c4));
+    }
+    const std::vector<int2> s1 = sorted(w1), s4 = sorted(w4);
+    SPK_TRY(upload_vec(c.w1, s1));
+    SPK_TRY(upload_vec(c.w4, s4));
+    c.n1 = (int)s1.size();
+    c.n4 = (int)s4.size();
+    // reduced solves: one argument block per virtual system that has a reduced system
+    SPK_TRY(upload_vec(c.red, red));
+    SPK_TRY(upload_vec(c.cred, cred));
+    c.nred = (int)red.size();
+    SPK_TRY(upload_vec(c.va, va));
+    SPK_TRY(upload_vec(c.vw, vw));
+    c.nvw = (int)vw.size();
+    return SPK_OK;
+}
+
+template <int K, typename T>
+void enqueue_solve(spk_group *g, GroupClass &c, bool correction, cudaStream_t st) {
+    const TileArgs *p1 = correction ? c.c1.p : c.a1.p;
+    const TileArgs *p4 = correction ? c.c4.p : c.a4.p;
+    if (c.n1) {
+        k_tile_multi<false, K, T, T><<<c.n1, 32, 0, st>>>(p1, c.w1.p);
+        g->kernels++;
+    }
+    if (c.nred) {
+        k_reduced_multi<K, T><<<c.nred, red_threads<K>(), 0, st>>>(c.red.p);
+        g->kernels++;
+    }
+    if (c.n4) {
+        k_tile_multi<true, K, T, double><<<c.n4, 32, 0, st>>>(p4, c.w4.p);
+        g->kernels++;
+    }
+}
+
+template <int K>
+void enqueue_class(spk_group *g, GroupClass &c, cudaStream_t st) {
+    if (g->mode == 0) {
+        enqueue_solve<K, double>(g, c, false, st);
+        return;
+    }
+    enqueue_solve<K, float>(g, c, false, st);
+    for (int it = 0; it < g->iters; it++) {
+        k_residual_multi<K><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 0);
+        enqueue_solve<K, float>(g, c, true, st);
+        k_axpy_multi<K><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p);
+        g->kernels += 2;
+    }
+}
+
+void enqueue_all(spk_group *g, cudaStream_t st) {
+    for (auto &c : g->cls) {
+        if (c.vs.empty()) continue;
+        switch (c.K) {
+            case 16: enqueue_class<16>(g, c, st); break;
+            case 8: enqueue_class<8>(g, c, st); break;
+            case 4: enqueue_class<4>(g, c, st); break;
+            case 2: enqueue_class<2>(g, c, st); break;
+            default: enqueue_class<1>(g, c, st); break;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace spk
+
+using namespace spk;
+
+extern "C" {
+
+int spk_group_destroy(spk_group *g) {
+    if (!g) return SPK_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return SPK_OK;
+}
+
+int spk_group_create(spk_group **out, int count, spk_system *const *systems, const int *nrhs,
+                     const double *const *B, const long long *ldb, double *const *X, const long long *ldx, int mode,
+                     int iters, void *stream) {
+    if (!out || count <= 0 || !systems || !nrhs || !B || !ldb || !X || !ldx || (mode != 0 && mode != 1) ||
+        iters < 0) {
+        set_error(SPK_ERR_ARG, "invalid group arguments (count=%d, mode=%d, iters=%d)", count, mode, iters);
+        return SPK_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    spk_group *g = new spk_group();
+    g->mode = mode;
+    g->iters = mode == 1 ? iters : 0;
+    auto fail = [&](int rc) {
+        spk_group_destroy(g);
+        return rc;
+    };
+    std::vector<std::vector<SegTask>> t1(count), t4(count);
+    long long cols = 0, pool_bytes = 0;
+    for (int i = 0; i < count; i++) {
+        spk_system *s = systems[i];
+        if (!s || !s->built || !s->ell_ok || nrhs[i] <= 0 || ldb[i] < s->n || ldx[i] < s->n || !B[i] || !X[i]) {
+            set_error(SPK_ERR_ARG, "group member %d: needs a preprocessed system on the sliced-ELL layout, nrhs > 0 "
+                                   "and leading dimensions >= n", i);
+            return fail(SPK_ERR_ARG);
+        }
+        if (mode == 1) {
+            int rc = ensure_fp32(s);
+            if (rc == SPK_OK) rc = ensure_residual(s);
+            if (rc != SPK_OK) return fail(rc);
+        } else if (!s->diag.p) {
+            const int rc = ensure_residual(s);
+            if (rc != SPK_OK) return fail(rc);
+        }
+        t1[i].resize(s->ntasks1);
+        t4[i].resize(s->ntasks2);
+        if (s->ntasks1 && cudaMemcpy(t1[i].data(), s->d_tasks1.p, sizeof(SegTask) * s->ntasks1,
+                                     cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(SPK_ERR_CUDA);
+        if (cudaMemcpy(t4[i].data(), s->d_tasks2.p, sizeof(SegTask) * s->ntasks2, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            return fail(SPK_ERR_CUDA);
+        g->sys.push_back(s);
+        // width classes: binary decomposition of nrhs in pieces of at most 16
+        int left = nrhs[i], col = 0;
+        while (left > 0) {
+            int K = 16;
+            while (K > left) K >>= 1;
+            GroupVS v{};
+            v.s = s;
+            v.sys = i;
+            v.K = K;
+            v.col0 = (int)cols;
+            v.B = B[i] + col * ldb[i];
+            v.ldb = ldb[i];
+            v.X = X[i] + col * ldx[i];
+            v.ldx = ldx[i];
+            const long long kn = (long long)K * s->n;
+            v.work = (char *)(intptr_t)pool_bytes;  // offsets until the pool exists
+            pool_bytes += ((kn * (mode == 1 ? 4 : 8)) + 255) / 256 * 256;
+            if (mode == 1) {
+                v.R = (double *)(intptr_t)pool_bytes;
+                pool_bytes += (kn * 8 + 255) / 256 * 256;
+                v.D = (double *)(intptr_t)pool_bytes;
+                pool_bytes += (kn * 8 + 255) / 256 * 256;
+            }
+            g->vs.push_back(v);
+            cols += K;
+            col += K;
+            left -= K;
+        }
+    }
+    if (g->pool.alloc(std::max<long long>(pool_bytes, 256)) != SPK_OK) return fail(SPK_ERR_NOMEM);
+    if (g->norms.alloc(3 * cols) != SPK_OK) return fail(SPK_ERR_NOMEM);
+    g->norm_cols = cols;
+    for (auto &v : g->vs) {
+        v.work = g->pool.p + (intptr_t)v.work;
+        if (mode == 1) {
+            v.R = (double *)(g->pool.p + (intptr_t)v.R);
+            v.D = (double *)(g->pool.p + (intptr_t)v.D);
+        }
+    }
+    for (int c = 0; c < 5; c++) g->cls[c].K = kGroupK[c];
+    for (int i = 0; i < (int)g->vs.size(); i++)
+        for (int c = 0; c < 5; c++)
+            if (g->vs[i].K == kGroupK[c]) g->cls[c].vs.push_back(i);
+    for (auto &c : g->cls) {
+        if (c.vs.empty()) continue;
+        const int rc = build_class(g, c, t1, t4);
+        if (rc != SPK_OK) return fail(rc);
+    }
+    // capture the launch sequence
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        (void)cudaGetLastError();  // not sticky: clear it for the caller's next checks
+        set_error(SPK_ERR_CUDA, "cudaStreamBeginCapture failed (a legacy default stream cannot be captured)");
+        return fail(SPK_ERR_CUDA);
+    }
+    enqueue_all(g, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g->graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        set_error(SPK_ERR_CUDA, "group graph capture failed: %s", cudaGetErrorString(e));
+        return fail(SPK_ERR_CUDA);
+    }
+    *out = g;
+    return SPK_OK;
+}
+
+int spk_group_solve(spk_group *g, void *stream) {
+    if (!g || !g->exec) {
+        set_error(SPK_ERR_ARG, "null group");
+        return SPK_ERR_ARG;
+    }
+    SPK_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return SPK_OK;
+}
+
+int spk_group_residual(spk_group *g, void *stream, double *worst) {
+    if (!g || !worst) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // residuals into the R buffers of FP32 groups, or a scratch pool for FP64 groups
+    DBuf<double> scratch;
+    if (g->mode == 0) {
+        long long maxkn = 0;
+        for (auto &v : g->vs) maxkn += (long long)v.K * v.s->n;
+        SPK_TRY(scratch.alloc(std::max<long long>(maxkn, 1)));
+        long long off = 0;
+        for (auto &c : g->cls) {
+            if (c.vs.empty()) continue;
+            std::vector<VecArgs> va(c.vs.size());
+            SPK_CUDA(cudaMemcpy(va.data(), c.va.p, sizeof(VecArgs) * va.size(), cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < va.size(); i++) {
+                va[i].R = scratch.p + off;
+                off += (long long)va[i].n * c.K;
+            }
+            SPK_CUDA(cudaMemcpy(c.va.p, va.data(), sizeof(VecArgs) * va.size(), cudaMemcpyHostToDevice));
+        }
+    }
+    SPK_CUDA(cudaMemsetAsync(g->norms.p, 0, sizeof(unsigned long long) * 3 * g->norm_cols, st));
+    for (auto &c : g->cls) {
+        if (c.vs.empty()) continue;
+        switch (c.K) {
+            case 16: k_residual_multi<16><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 1); break;
+            case 8: k_residual_multi<8><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 1); break;
+            case 4: k_residual_multi<4><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 1); break;
+            case 2: k_residual_multi<2><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 1); break;
+            default: k_residual_multi<1><<<c.nvw, 256, 0, st>>>(c.va.p, c.vw.p, 1); break;
+        }
+        SPK_CUDA(cudaGetLastError());
+    }
+    std::vector<unsigned long long> h(3 * g->norm_cols);
+    SPK_CUDA(cudaMemcpyAsync(h.data(), g->norms.p, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
+    SPK_CUDA(cudaStreamSynchronize(st));
+    double w = 0.0;
+    for (auto &v : g->vs)
+        for (int k = 0; k < v.K; k++) {
+            double nr, nx, nb;
+            memcpy(&nr, &h[3 * (v.col0 + k)], 8);
+            memcpy(&nx, &h[3 * (v.col0 + k) + 1], 8);
+            memcpy(&nb, &h[3 * (v.col0 + k) + 2], 8);
+            const double den = v.s->anorm * nx + nb;
+            w = std::max(w, den > 0 ? nr / den : nr);
+        }
+    *worst = w;
+    for (auto *s : g->sys) SPK_TRY(check_device_error(s));
+    return SPK_OK;
+}
+
+long long spk_group_info(const spk_group *g, const char *name) {
+    if (!g || !name) return -1;
+    if (!strcmp(name, "kernels")) return g->kernels;
+    if (!strcmp(name, "virtual_systems")) return (long long)g->vs.size();
+    if (!strcmp(name, "columns")) return g->norm_cols;
+    long long items = 0;
+    for (auto &c : g->cls) items += c.n1 + c.n4;
+    if (!strcmp(name, "task_items")) return items;
+    if (!strcmp(name, "pool_bytes")) return (long long)g->pool.n;
+    return -1;
+}
+
+}  // extern "C"
