@@ -239,7 +239,8 @@ int spk_group_destroy(spk_group *g);
  * while other batches run join the next batch and batches of different
  * matrices overlap on the device.  Requests take host arrays (column-major,
  * leading dimension n) that must stay valid until spk_server_wait returns.
- * SPK_MODE_FP32_IR requests iterate to scaled residual <= 1e-12. */
+ * SPK_MODE_FP32_IR requests iterate to scaled residual <= 1e-12; every batch's
+ * scaled residual is checked against 1e-12. */
 typedef struct spk_server spk_server;
 int spk_server_create(spk_server **out, long long hbm_budget_bytes, int nslots);
 int spk_server_destroy(spk_server *srv);
@@ -253,8 +254,11 @@ int spk_server_submit(spk_server *srv, int id, int nrhs, const double *b, double
  * batch's right-hand-side count. */
 int spk_server_wait(spk_server *srv, long long ticket, double *latency_s, double *resid, int *iters,
                     int *batch_rhs);
-/* out[0..8]: resident bytes, staging bytes, resident systems, evictions,
- * preprocessings, batches, right-hand sides batched, requests completed, budget. */
+/* out[0..10]: resident bytes, staging bytes, resident systems, evictions,
+ * preprocessings, batches, right-hand sides batched, requests completed, budget,
+ * batches retried after releasing idle systems when device memory ran out,
+ * batches solved again in FP64 because their scaled residual was above 1e-12
+ * (requests still above it fail with SPK_ERR_INPUT). */
 int spk_server_stats(spk_server *srv, long long *out, int count);
 
 /* The system used by the Part-1 entry points (NULL before the first preproc). */

@@ -24,6 +24,7 @@
 // * Each request records its latency (submit to result in host memory) and the
 //   scaled residual of its batch.
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -39,6 +40,7 @@
 namespace {
 
 constexpr int kBatchRhs = 32;
+constexpr double kTol = 1e-12;  // scaled residual every served result must reach
 
 double wall_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -61,6 +63,7 @@ struct Matrix {
     std::vector<int> ia, ja;
     spk_system *sys = nullptr;
     long long bytes = 0;      // device footprint while resident
+    long long known = 0;      // footprint last measured (kept across evictions)
     long long last_use = 0;   // LRU clock
     bool busy = false;        // in a batch (or being preprocessed)
     std::deque<Request *> pending;
@@ -85,7 +88,8 @@ struct spk_server {
     std::unordered_map<long long, Request *> reqs;
     std::vector<Slot *> slots;
     long long next_ticket = 1, clock = 0;
-    long long evictions = 0, preprocs = 0, batches = 0, batched_rhs = 0, completed = 0;
+    long long evictions = 0, preprocs = 0, batches = 0, batched_rhs = 0, completed = 0, nomem_retries = 0;
+    long long rechecks = 0;
     int device = 0;
     bool stop = false;
 };
@@ -112,11 +116,13 @@ int copy_csr(Matrix *M, const double *a, const int *ia, const int *ja, int n) {
     return SPK_OK;
 }
 
-// Device footprint estimate before preprocessing: the CSR copy, the ELL copy,
-// the spike/reduced pools and one batch of work buffers scale with nnz and n.
+// Device footprint for admission: the last measured one, else an estimate (the
+// CSR and ELL copies and pools ~64 B per nonzero, dense spikes up to ~1 KB per
+// row, one batch of work buffers 3 x 32 x 8 B per row).
 long long estimate_bytes(const Matrix *M) {
+    if (M->known > 0) return M->known;
     const long long nnz = (long long)M->a.size(), n = M->n;
-    return 40 * nnz + 64 * n + (long long)kBatchRhs * 8 * 3 * n;
+    return 64 * nnz + 1024 * n + (long long)kBatchRhs * 8 * 3 * n;
 }
 
 // Destroy idle resident systems, least recently used first, until `need` more
@@ -174,10 +180,10 @@ int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch,
         c += r->nrhs;
     }
     SPK_CUDA(cudaMemcpyAsync(sl->dB, sl->hB, sizeof(double) * k * n, cudaMemcpyHostToDevice, sl->st));
-    // FP32 + refinement iterates to scaled residual <= 1e-12 (and reports it);
-    // FP64 batches skip the residual pass
-    SPK_TRY(spk_solve_batch(M->sys, k, sl->dB, n, sl->dX, n, mode, mode == SPK_MODE_FP32_IR ? 1e-12 : -1.0, 10,
-                            (void *)sl->st, iters, mode == SPK_MODE_FP32_IR ? resid : nullptr));
+    // FP32 + refinement iterates to scaled residual <= 1e-12; every batch reports
+    // its scaled residual (the caller checks it)
+    SPK_TRY(spk_solve_batch(M->sys, k, sl->dB, n, sl->dX, n, mode, mode == SPK_MODE_FP32_IR ? kTol : -1.0, 10,
+                            (void *)sl->st, iters, resid));
     SPK_CUDA(cudaMemcpyAsync(sl->hX, sl->dX, sizeof(double) * k * n, cudaMemcpyDeviceToHost, sl->st));
     SPK_CUDA(cudaStreamSynchronize(sl->st));
     SPK_TRY(spk_check(M->sys));
@@ -254,7 +260,7 @@ void worker(spk_server *S, Slot *sl) {
         double resid = -1;
         const double t0 = wall_s();
         for (Request *r : batch) r->t_start = t0;
-        if (status == SPK_OK) {
+        for (int attempt = 0; status == SPK_OK && attempt < 2; attempt++) {
             lk.unlock();
             status = run_batch(S, sl, M, batch, mode, &iters, &resid);
             lk.lock();
@@ -262,6 +268,25 @@ void worker(spk_server *S, Slot *sl) {
             const long long now = spk_debug_scalar(M->sys, "device_bytes");
             S->resident += now - M->bytes;
             M->bytes = now;
+            M->known = std::max(M->known, now);
+            if (status == SPK_OK && !(resid >= 0 && resid <= kTol)) {
+                // not at the tolerance (FP32 refinement that stalls, or a bad
+                // batch): solve it again in FP64 and check; fail it if still above
+                lk.unlock();
+                status = run_batch(S, sl, M, batch, SPK_MODE_FP64, &iters, &resid);
+                lk.lock();
+                S->rechecks++;
+                if (status == SPK_OK && !(resid >= 0 && resid <= kTol)) {
+                    set_error(SPK_ERR_INPUT, "batch scaled residual %.3e above %.0e", resid, kTol);
+                    status = SPK_ERR_INPUT;
+                }
+            }
+            if (status != SPK_ERR_NOMEM || attempt == 1) break;
+            // device memory ran out (other workers' preprocessing or staging):
+            // release every idle system and retry once
+            make_room(S, S->budget, M);
+            S->nomem_retries++;
+            status = SPK_OK;
         }
         const double t1 = wall_s();
         for (Request *r : batch) {
@@ -432,9 +457,9 @@ int spk_server_stats(spk_server *S, long long *out, int count) {
     std::lock_guard<std::mutex> g(S->mu);
     long long nres = 0;
     for (auto &kv : S->mats) nres += kv.second->sys != nullptr;
-    const long long v[9] = {S->resident, S->workspace, nres, S->evictions, S->preprocs,
-                            S->batches, S->batched_rhs, S->completed, S->budget};
-    for (int i = 0; i < count && i < 9; i++) out[i] = v[i];
+    const long long v[11] = {S->resident, S->workspace, nres, S->evictions, S->preprocs,     S->batches,
+                             S->batched_rhs, S->completed, S->budget,   S->nomem_retries, S->rechecks};
+    for (int i = 0; i < count && i < 11; i++) out[i] = v[i];
     return SPK_OK;
 }
 

@@ -1142,6 +1142,10 @@ __global__ void k_aux_first(int rows, int ncols, const double *__restrict__ W, d
     if (s > tau) atomicMin(first, r);
 }
 
+// max(m, v) for norms that must not lose a NaN: once either operand is NaN the
+// result is NaN (fmax would drop it and let a failed solve look converged)
+__device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
+
 // ---- batched solve support --------------------------------------------------------
 
 // Reduced solve on the kept rows for K right-hand sides stored in T with FP64
@@ -1276,9 +1280,9 @@ __global__ void __launch_bounds__(256) k_residual_multi(const VecArgs *__restric
         }
 #pragma unroll
         for (int s = 16; s; s >>= 1) {
-            mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, s));
-            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, s));
-            mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, s));
+            mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, s));
+            mx = nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+            mb = nanmax(mb, __shfl_xor_sync(0xffffffffu, mb, s));
         }
         if ((threadIdx.x & 31) == 0) {
             atomicMax(&A.norms[3 * k + 0], __double_as_longlong(mr));
@@ -1419,9 +1423,9 @@ k_rhs_residual(int n, int nk, const int *__restrict__ ptr, const double *__restr
                 const double b = S.bt[l][lane];
                 const double res = b - fma(S.dg[l], xr, (a[0] + a[1]) + (a[2] + a[3]));
                 S.bt[l][lane] = res;
-                mr = fmax(mr, fabs(res));
-                mx = fmax(mx, fabs(xr));
-                mb = fmax(mb, fabs(b));
+                mr = nanmax(mr, fabs(res));
+                mx = nanmax(mx, fabs(xr));
+                mb = nanmax(mb, fabs(b));
             }
         } else
         for (int l = warp; l < rows; l += kResWarps) {
@@ -1449,9 +1453,9 @@ k_rhs_residual(int n, int nk, const int *__restrict__ ptr, const double *__restr
             const double b = S.bt[l][lane];
             const double res = b - fma(S.dg[l], xr, a0 + a1);
             S.bt[l][lane] = res;
-            mr = fmax(mr, fabs(res));
-            mx = fmax(mx, fabs(xr));
-            mb = fmax(mb, fabs(b));
+            mr = nanmax(mr, fabs(res));
+            mx = nanmax(mx, fabs(xr));
+            mb = nanmax(mb, fabs(b));
         }
         __syncthreads();
         if (lane < rows) {
@@ -1498,15 +1502,15 @@ __global__ void k_norms(int n, int nrhs, const double *__restrict__ R, long long
     const int k = blockIdx.y;
     double mr = 0, mx = 0, mb = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        mr = fmax(mr, fabs(R[k * ldr + i]));
-        mx = fmax(mx, fabs(X[k * ldx + i]));
-        mb = fmax(mb, fabs(B[k * ldb + i]));
+        mr = nanmax(mr, fabs(R[k * ldr + i]));
+        mx = nanmax(mx, fabs(X[k * ldx + i]));
+        mb = nanmax(mb, fabs(B[k * ldb + i]));
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
-        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
-        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+        mr = nanmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        mx = nanmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mb = nanmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
     }
     if ((threadIdx.x & 31) == 0) {
         atomicMax(&out[3 * k + 0], __double_as_longlong(mr));
@@ -1988,6 +1992,9 @@ void launch_residual(spk_system *s, const double *X, long long ldx, const double
                                                      B, ldb, R, ldr, s->uplo == 'L');
 }
 
+// max for scaled residuals that keeps a NaN (std::max would drop it)
+inline double worst_of(double w, double v) { return (v > w || v != v) ? v : w; }
+
 // R = B - A X (FP64) for K right-hand sides; with norms, also the per-column
 // max |R|, |X|, |B| in d_norms (read back by scaled_residual).
 int residual(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
@@ -2032,7 +2039,7 @@ int scaled_residual(spk_system *s, int K, cudaStream_t st, double *out) {
         memcpy(&nx, &h[3 * k + 1], 8);
         memcpy(&nb, &h[3 * k + 2], 8);
         const double den = s->anorm * nx + nb;
-        worst = std::max(worst, den > 0 ? nr / den : nr);
+        worst = worst_of(worst, den > 0 ? nr / den : nr);
     }
     *out = worst;
     return SPK_OK;
@@ -2195,7 +2202,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                 SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st, true));
                 double r = 0;
                 SPK_TRY(scaled_residual(s, K, st, &r));
-                worst = std::max(worst, r);
+                worst = worst_of(worst, r);
             }
         } else {
             SPK_TRY(ensure_work(s, sizeof(float) * wcols * n));
@@ -2226,7 +2233,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                 }
             }
             max_it = std::max(max_it, it);
-            if (r >= 0) worst = std::max(worst, r);
+            if (!(r < 0)) worst = worst_of(worst, r);
         }
         g += K;
     }
@@ -2755,7 +2762,7 @@ int spk_group_residual(spk_group *g, void *stream, double *worst) {
             memcpy(&nx, &h[3 * (v.col0 + k) + 1], 8);
             memcpy(&nb, &h[3 * (v.col0 + k) + 2], 8);
             const double den = v.s->anorm * nx + nb;
-            w = std::max(w, den > 0 ? nr / den : nr);
+            w = worst_of(w, den > 0 ? nr / den : nr);
         }
     *worst = w;
     for (auto *s : g->sys) SPK_TRY(check_device_error(s));

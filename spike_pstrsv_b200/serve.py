@@ -18,7 +18,7 @@ from .capi import SpkError, lib
 MODE_FP64 = 0
 MODE_FP32_IR = 1
 STATS = ("resident_bytes", "staging_bytes", "resident_systems", "evictions", "preprocessings", "batches",
-         "rhs_batched", "completed", "budget")
+         "rhs_batched", "completed", "budget", "nomem_retries", "rechecks")
 
 _bound = False
 
@@ -49,7 +49,7 @@ def _check(rc: int):
 class Result:
     x: np.ndarray          # (nrhs, n) solutions
     latency_s: float       # submit to result in host memory
-    scaled_residual: float  # of the request's batch (FP32+IR; -1 for FP64)
+    scaled_residual: float  # of the request's batch
     refinement_steps: int
     batch_rhs: int         # right-hand sides in the batch that served it
 

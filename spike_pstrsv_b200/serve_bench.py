@@ -95,7 +95,10 @@ def run_stream(pool, rate: float, nreq: int, budget: int, slots: int, mode: int,
             for j in range(nreq):
                 while tickets[j] is None:
                     time.sleep(0)
-                results[j] = tickets[j].wait()
+                try:
+                    results[j] = tickets[j].wait()
+                except Exception as e:  # a failed request is counted, the stream goes on
+                    results[j] = e
             done.set()
 
         th = threading.Thread(target=collect)
@@ -128,22 +131,35 @@ def run_stream(pool, rate: float, nreq: int, budget: int, slots: int, mode: int,
         th.join()
         t_end = time.perf_counter()
         stats = S.stats()
+    failed = [j for j, r in enumerate(results) if isinstance(r, Exception)]
+    errors = sorted({str(results[j]) for j in failed})[:3]
+    keep = [j for j in range(nreq) if j not in set(failed)]
+    results = [results[j] for j in keep]
+    meta = [meta[j] for j in keep]
+    plan = [plan[j] for j in keep]
     lat = np.array([r.latency_s + m[2] for r, m in zip(results, meta)])
     solve_lat = np.array([r.latency_s for r, m, p in zip(results, meta, plan) if p[0] == "solve"])
     rhs = sum(m[1] for m in meta)
     worst_res = max(r.scaled_residual for r in results)
     err = 0.0
-    for r, m in zip(results, meta):
+    wrong = []
+    for r, m, pl in zip(results, meta, plan):
         Xt = pool[m[0]]["X"][:m[1]]
-        err = max(err, float(np.abs(r.x - Xt).max() / np.abs(Xt).max()))
+        e = float(np.abs(r.x - Xt).max() / np.abs(Xt).max())
+        err = max(err, e)
+        if e > 1e-10:
+            wrong.append({"matrix": m[0], "m": pool[m[0]]["L"].m, "kind": pl[0], "rhs": m[1],
+                          "batch_rhs": r.batch_rhs, "resid": r.scaled_residual, "steps": r.refinement_steps,
+                          "rel_err": e})
     wall = t_end - t_start
-    return {"offered_req_per_s": rate, "requests": nreq, "rhs": int(rhs), "wall_s": wall,
+    return {"offered_req_per_s": rate, "requests": nreq, "failed": len(failed), "failures": errors,
+            "rhs": int(rhs), "wall_s": wall,
             "solves_per_s": rhs / wall, "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "solve_p50_ms": float(np.percentile(solve_lat, 50) * 1e3),
             "solve_p99_ms": float(np.percentile(solve_lat, 99) * 1e3), "mean_batch_rhs": stats["rhs_batched"] / max(stats["batches"], 1),
             "uploads": sum(1 for p in plan if p[0] == "upload"), "max_scaled_residual": worst_res,
-            "max_rel_err_vs_x_true": err, "server": stats, "plan": [(m[0], m[1]) for m in meta]}
+            "max_rel_err_vs_x_true": err, "wrong_results": wrong[:20], "n_wrong": len(wrong), "server": stats, "plan": [(m[0], m[1]) for m in meta]}
 
 
 def run(full: bool = False, rates=(50.0, 150.0, 500.0, 2000.0), nreq: int | None = None, slots: int = 4, seed: int = 0,

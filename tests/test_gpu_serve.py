@@ -125,3 +125,46 @@ def test_server_errors():
         _, B = synth.make_rhs(L, seed=0)
         r = S.submit(0, B).wait()
         assert r.scaled_residual <= TOL
+
+
+def test_batches_above_the_tolerance_are_solved_again_in_fp64():
+    """Values beyond the FP32 range (|a| ~ 1e39): the FP32 solve overflows, its
+    residual is NaN (not 'converged'), and the server re-solves the batch in FP64,
+    which meets the tolerance."""
+    n = 64
+    ia = np.zeros(n + 1, dtype=np.int32)
+    ja, a = [], []
+    for i in range(n):
+        if i:
+            ja.append(i - 1)
+            a.append(-1e38)
+        ja.append(i)
+        a.append(1e39)
+        ia[i + 1] = len(ja)
+    L = synth.CSR(n, ia, np.asarray(ja, np.int32), np.asarray(a))
+    Xt, B = synth.make_rhs(L, seed=0, nrhs=2)
+    with serve.Server(hbm_budget_bytes=1 << 30, slots=1) as S:
+        S.put_matrix(0, L.a, L.ia, L.ja, n, 2, "L")
+        r = S.submit(0, B, serve.MODE_FP32_IR).wait()
+        st = S.stats()
+    assert st["rechecks"] >= 1
+    assert 0 <= r.scaled_residual <= TOL
+    assert _rel(r.x, Xt) <= 1e-12
+
+
+def test_fp32_batch_reports_a_nan_residual_when_the_values_overflow():
+    import torch
+    import spike_pstrsv_b200 as spk
+    n = 64
+    ia = np.concatenate([[0], np.cumsum([1] + [2] * (n - 1))]).astype(np.int32)
+    ja = np.concatenate([[0]] + [[i - 1, i] for i in range(1, n)]).astype(np.int32)
+    a = np.concatenate([[1e39]] + [[-1e38, 1e39] for _ in range(1, n)])
+    L = synth.CSR(n, ia, ja, a)
+    _, B = synth.make_rhs(L, seed=1, nrhs=3)
+    S = spk.System().preproc(L.a, L.ia, L.ja, n, 2, "L", 1)
+    dB = torch.from_numpy(B).cuda()
+    dX = torch.zeros_like(dB)
+    it, r = S.solve_batch(dB, dX, mode=1, tol=1e-12, maxit=3)
+    assert not (r <= 1e-12)  # NaN or large: never reported as converged
+    it, r = S.solve_batch(dB, dX, mode=0)
+    assert r <= 1e-12
