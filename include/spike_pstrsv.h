@@ -159,6 +159,18 @@ enum { SPK_MODE_FP64 = 0, SPK_MODE_FP32_IR = 1 };
 int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
                     double tol, int maxit, void *stream, int *iters, double *resid);
 
+/* Lend the system device memory for the batched solves' work columns (no
+ * reference counterpart): with a workspace set, spk_solve_batch carves its
+ * work, residual and correction columns (32 x n FP64 each, as needed) from it
+ * instead of buffers it allocates and keeps with the system, and the system's
+ * own batch buffers are released.  spk_workspace_bytes gives the size a mode
+ * needs (mode SPK_MODE_FP64 or SPK_MODE_FP32_IR; with_residual: FP64 batches
+ * that report their residual).  One workspace can serve many systems whose
+ * batches do not overlap on the GPU; NULL, 0 detaches it.  256-byte aligned
+ * device memory; a batch that needs more returns SPK_ERR_TOO_LARGE. */
+int spk_set_workspace(spk_system *s, void *dev_ptr, long long bytes);
+long long spk_workspace_bytes(const spk_system *s, int mode, int with_residual);
+
 /* Batched FP64 solve that allocates no device memory; no counterpart in the
  * reference.  For callers that must not allocate once they are serving: a
  * process whose HBM is already committed under a fixed budget (where a new

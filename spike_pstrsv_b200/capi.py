@@ -63,6 +63,9 @@ def lib() -> ctypes.CDLL:
         L.spk_set_profiling.argtypes = [vp, i]
         L.spk_solve_batch.argtypes = [vp, i, vp, ctypes.c_longlong, vp, ctypes.c_longlong, i, d, i, vp,
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+        L.spk_set_workspace.argtypes = [vp, vp, ctypes.c_longlong]
+        L.spk_workspace_bytes.argtypes = [vp, i, i]
+        L.spk_workspace_bytes.restype = ctypes.c_longlong
         L.spk_phase_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
         _lib = L
     return _lib
@@ -247,6 +250,20 @@ class System:
                                      int(maxit), ctypes.c_void_p(stream), ctypes.byref(it),
                                      ctypes.byref(r) if want_resid else None))
         return it.value, (r.value if want_resid else None)
+
+    def set_workspace(self, ws=None) -> "System":
+        """Lend device memory (a CUDA tensor, 256-byte aligned) for the batched
+        solves' work columns; None detaches it."""
+        if ws is None:
+            _check(lib().spk_set_workspace(self.h, None, 0))
+        else:
+            _check(lib().spk_set_workspace(self.h, ctypes.c_void_p(ws.data_ptr()),
+                                           int(ws.numel() * ws.element_size())))
+        self._ws = ws
+        return self
+
+    def workspace_bytes(self, mode: int = 1, with_residual: bool = True) -> int:
+        return int(lib().spk_workspace_bytes(self.h, int(mode), int(with_residual)))
 
     def set_profiling(self, on: bool = True) -> "System":
         _check(lib().spk_set_profiling(self.h, int(on)))

@@ -3,6 +3,7 @@
 // handle-based spk_* extension.
 #include <cstdarg>
 #include <ctime>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -348,17 +349,17 @@ int spk_solve(spk_system *s, const double *b, double *x) {
     }
     int n = s->n;
     int bd = is_device_pointer(b), xd = is_device_pointer(x);
-    DBuf<double> tb, tx;
+    // host arrays go through device copies kept with the system (allocated once)
     const double *db = b;
     double *dx = x;
     if (!bd) {
-        SPK_TRY(tb.alloc(n));
-        SPK_CUDA(cudaMemcpyAsync(tb.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
-        db = tb.p;
+        if (s->stage_b.n < (size_t)n) SPK_TRY(s->stage_b.alloc(n));
+        SPK_CUDA(cudaMemcpyAsync(s->stage_b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
+        db = s->stage_b.p;
     }
     if (!xd) {
-        SPK_TRY(tx.alloc(n));
-        dx = tx.p;
+        if (s->stage_x.n < (size_t)n) SPK_TRY(s->stage_x.alloc(n));
+        dx = s->stage_x.p;
     }
     SPK_TRY(solve(s, db, dx, s->stream, nullptr));
     if (!xd) SPK_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
@@ -399,6 +400,32 @@ int spk_solve_batch_noalloc(spk_system *s, int nrhs, const double *B, long long 
         return SPK_ERR_ARG;
     }
     return solve_batch_static(s, nrhs, B, ldb, X, ldx, (cudaStream_t)stream);
+}
+
+int spk_set_workspace(spk_system *s, void *dev_ptr, long long bytes) {
+    if (!s || bytes < 0 || (dev_ptr && !is_device_pointer(dev_ptr)) || (!dev_ptr && bytes)) {
+        set_error(SPK_ERR_ARG, "invalid workspace (pointer %p, %lld bytes)", dev_ptr, bytes);
+        return SPK_ERR_ARG;
+    }
+    if (dev_ptr && ((uintptr_t)dev_ptr & 255)) {
+        set_error(SPK_ERR_ARG, "workspace must be 256-byte aligned");
+        return SPK_ERR_ARG;
+    }
+    s->ext_ws = (char *)dev_ptr;
+    s->ext_ws_bytes = dev_ptr ? (size_t)bytes : 0;
+    if (dev_ptr) {
+        // the system's own batch buffers are no longer needed
+        s->work.release();
+        s->rbuf.release();
+        s->dbuf.release();
+    }
+    return SPK_OK;
+}
+
+long long spk_workspace_bytes(const spk_system *s, int mode, int with_residual) {
+    if (!s) return -1;
+    const long long col = ((32ll * s->n * 8) + 255) / 256 * 256;
+    return col * (1 + (mode == 1 || with_residual) + (mode == 1));
 }
 
 int spk_set_profiling(spk_system *s, int on) {
@@ -466,6 +493,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->xout_u.bytes() + s->d_tasks1.bytes() + s->d_tasks2.bytes() + s->d_red_rows.bytes();
         b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
         b += s->ell_valf.bytes() + s->rdiagf.bytes() + s->diag.bytes() + s->rbuf.bytes() + s->dbuf.bytes() + s->work.bytes();
+        b += s->stage_b.bytes() + s->stage_x.bytes();
         return b;
     }
     return -1;

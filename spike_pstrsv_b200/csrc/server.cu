@@ -73,6 +73,7 @@ struct Slot {
     cudaStream_t st = nullptr;
     double *dB = nullptr, *dX = nullptr, *hB = nullptr, *hX = nullptr;
     size_t cap = 0;  // doubles in each buffer
+    spk::DBuf<char> ws;  // batch work columns, lent to the system being solved
     std::thread th;
 };
 
@@ -167,13 +168,28 @@ int ensure_slot_capacity(spk_server *S, Slot *sl, size_t doubles) {
     return SPK_OK;
 }
 
-// Copy-in, batched solve and copy-out of one batch on the slot's stream.
+// The slot's workspace, grown to what a batch on this system needs.
+int ensure_slot_workspace(spk_server *S, Slot *sl, spk_system *sys) {
+    const long long need = spk_workspace_bytes(sys, SPK_MODE_FP32_IR, 1);
+    if ((long long)sl->ws.n >= need) return SPK_OK;
+    const long long old = (long long)sl->ws.n;
+    SPK_TRY(sl->ws.alloc((size_t)need));
+    std::lock_guard<std::mutex> g(S->mu);
+    S->workspace += need - old;
+    return SPK_OK;
+}
+
+// Copy-in, batched solve and copy-out of one batch on the slot's stream; the
+// system borrows the slot's workspace for the batch (resident systems keep no
+// batch buffers).
 int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch, int mode, int *iters,
               double *resid) {
     const long long n = M->n;
     int k = 0;
     for (Request *r : batch) k += r->nrhs;
     SPK_TRY(ensure_slot_capacity(S, sl, (size_t)k * n));
+    SPK_TRY(ensure_slot_workspace(S, sl, M->sys));
+    SPK_TRY(spk_set_workspace(M->sys, sl->ws.p, (long long)sl->ws.n));
     int c = 0;
     for (Request *r : batch) {
         memcpy(sl->hB + (size_t)c * n, r->b, sizeof(double) * r->nrhs * n);
@@ -182,10 +198,13 @@ int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch,
     SPK_CUDA(cudaMemcpyAsync(sl->dB, sl->hB, sizeof(double) * k * n, cudaMemcpyHostToDevice, sl->st));
     // FP32 + refinement iterates to scaled residual <= 1e-12; every batch reports
     // its scaled residual (the caller checks it)
-    SPK_TRY(spk_solve_batch(M->sys, k, sl->dB, n, sl->dX, n, mode, mode == SPK_MODE_FP32_IR ? kTol : -1.0, 10,
-                            (void *)sl->st, iters, resid));
-    SPK_CUDA(cudaMemcpyAsync(sl->hX, sl->dX, sizeof(double) * k * n, cudaMemcpyDeviceToHost, sl->st));
-    SPK_CUDA(cudaStreamSynchronize(sl->st));
+    const int rc = spk_solve_batch(M->sys, k, sl->dB, n, sl->dX, n, mode, mode == SPK_MODE_FP32_IR ? kTol : -1.0, 10,
+                                   (void *)sl->st, iters, resid);
+    if (rc == SPK_OK) SPK_CUDA(cudaMemcpyAsync(sl->hX, sl->dX, sizeof(double) * k * n, cudaMemcpyDeviceToHost, sl->st));
+    const cudaError_t e = cudaStreamSynchronize(sl->st);
+    spk_set_workspace(M->sys, nullptr, 0);
+    if (rc != SPK_OK) return rc;
+    SPK_CUDA(e);
     SPK_TRY(spk_check(M->sys));
     c = 0;
     for (Request *r : batch) {
@@ -345,6 +364,7 @@ int spk_server_destroy(spk_server *S) {
     for (Slot *sl : S->slots)
         if (sl->th.joinable()) sl->th.join();
     for (Slot *sl : S->slots) {
+        sl->ws.release();
         if (sl->dB) cudaFree(sl->dB);
         if (sl->dX) cudaFree(sl->dX);
         if (sl->hB) cudaFreeHost(sl->hB);

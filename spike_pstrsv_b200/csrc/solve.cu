@@ -2165,16 +2165,40 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     const long long n = s->n;
     int max_it = 0;
     double worst = 0.0;
+    // work columns (up to 32 x n, FP64 or FP32), residual and correction columns
+    // (32 x n FP64 each): from the caller's workspace when one is set, else the
+    // system's own buffers, grown on demand
+    const bool need_r = mode == 1 || resid, need_d = mode == 1;
+    const size_t col_bytes = ((size_t)32 * n * sizeof(double) + 255) / 256 * 256;
+    char *work_p = nullptr;
+    double *rbuf_p = nullptr, *dbuf_p = nullptr;
     if (mode == 1) {
         SPK_TRY(ensure_fp32(s));
-        SPK_TRY(ensure_residual(s));
         SPK_TRY(ensure_reach(s));
-        if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
-        if (s->dbuf.n < (size_t)(32 * n)) SPK_TRY(s->dbuf.alloc(32 * n));
-    } else if (resid) {
-        SPK_TRY(ensure_residual(s));
-        if (s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
     }
+    if (need_r) SPK_TRY(ensure_residual(s));
+    if (s->ext_ws) {
+        const size_t need = col_bytes * (1 + need_r + need_d);
+        if (s->ext_ws_bytes < need) {
+            set_error(SPK_ERR_TOO_LARGE, "workspace of %zu bytes is below the %zu this batch needs", s->ext_ws_bytes,
+                      need);
+            return SPK_ERR_TOO_LARGE;
+        }
+        work_p = s->ext_ws;
+        if (need_r) rbuf_p = (double *)(s->ext_ws + col_bytes);
+        if (need_d) dbuf_p = (double *)(s->ext_ws + 2 * col_bytes);
+    } else {
+        if (need_r && s->rbuf.n < (size_t)(32 * n)) SPK_TRY(s->rbuf.alloc(32 * n));
+        if (need_d && s->dbuf.n < (size_t)(32 * n)) SPK_TRY(s->dbuf.alloc(32 * n));
+        rbuf_p = s->rbuf.p;
+        dbuf_p = s->dbuf.p;
+    }
+    auto work_for = [&](size_t bytes) -> int {
+        if (s->ext_ws) return SPK_OK;
+        SPK_TRY(ensure_work(s, bytes));
+        work_p = s->work.p;
+        return SPK_OK;
+    };
     // The right-hand-side-parallel solver runs one warp per task along the task's
     // rows; it pays off once the tasks fill the GPU (two per SM).  With fewer
     // tasks the tile solver (rows of a tile across the lanes) has the shorter path.
@@ -2193,20 +2217,20 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
         const double *Bg = B + g * ldb;
         double *Xg = X + g * ldx;
         if (mode == 0) {
-            SPK_TRY(ensure_work(s, sizeof(double) * wcols * n));
+            SPK_TRY(work_for(sizeof(double) * wcols * n));
             if (rhs_path)
-                SPK_TRY(launch_rhs<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
+                SPK_TRY(launch_rhs<double>(s, K, Bg, ldb, Xg, ldx, (double *)work_p, st));
             else
-                SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)s->work.p, st));
+                SPK_TRY(launch_tiles_k<double>(s, K, Bg, ldb, Xg, ldx, (double *)work_p, st));
             if (resid) {
-                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st, true));
+                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, rbuf_p, n, st, true));
                 double r = 0;
                 SPK_TRY(scaled_residual(s, K, st, &r));
                 worst = worst_of(worst, r);
             }
         } else {
-            SPK_TRY(ensure_work(s, sizeof(float) * wcols * n));
-            float *wk = (float *)s->work.p;
+            SPK_TRY(work_for(sizeof(float) * wcols * n));
+            float *wk = (float *)work_p;
             auto solve32 = [&](const double *rhs, long long ld, double *xo, long long ldo) {
                 return rhs_path ? launch_rhs<float>(s, K, rhs, ld, xo, ldo, wk, st)
                                : launch_tiles_k<float>(s, K, rhs, ld, xo, ldo, wk, st);
@@ -2217,7 +2241,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
             for (;; it++) {
                 const bool check = tol >= 0 || (resid && it == maxit);
                 if (tol < 0 && it == maxit && !resid) break;
-                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, s->rbuf.p, n, st, check));
+                SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, rbuf_p, n, st, check));
                 if (check) {
                     SPK_TRY(scaled_residual(s, K, st, &r));
                     if ((tol >= 0 && r <= tol) || it == maxit) break;
@@ -2225,10 +2249,10 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                 if (it == maxit) break;
                 if (rhs_path && s->ell_reach < kRhsWin) {
                     // correction added in place by phase 3+4 (no coupling leaves the window)
-                    SPK_TRY(launch_rhs<float>(s, K, s->rbuf.p, n, Xg, ldx, wk, st, true));
+                    SPK_TRY(launch_rhs<float>(s, K, rbuf_p, n, Xg, ldx, wk, st, true));
                 } else {
-                    SPK_TRY(solve32(s->rbuf.p, n, s->dbuf.p, n));
-                    k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, s->dbuf.p, Xg, ldx);
+                    SPK_TRY(solve32(rbuf_p, n, dbuf_p, n));
+                    k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, dbuf_p, Xg, ldx);
                     SPK_CUDA(cudaGetLastError());
                 }
             }

@@ -141,7 +141,10 @@ struct spk_system {
     spk::DBuf<char> work;
     spk::DBuf<unsigned long long> d_norms;
     double anorm = 0.0;
-    int ell_reach = -1;  // largest column distance from a tile's first row (-1: not computed)
+    int ell_reach = -1;
+    spk::DBuf<double> stage_b, stage_x;  // device copies of host b / x for spk_solve
+    char *ext_ws = nullptr;  // caller-lent device workspace for the batched solves (spk_set_workspace)
+    size_t ext_ws_bytes = 0;  // largest column distance from a tile's first row (-1: not computed)
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     // optional per-phase device timing (spk_set_profiling)

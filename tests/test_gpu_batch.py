@@ -117,3 +117,29 @@ def test_batch_paths_agree(nparts):
     for k in range(24):
         assert rel_err(X[k], Xt[k]) <= 1e-12
         assert rel_err(X[k], S.solve(B[k])) <= 1e-13
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_with_a_lent_workspace(mode):
+    """Work columns carved from caller memory give the same answer as the
+    system's own buffers; a workspace below the need is refused."""
+    import torch
+    L = synth.banded_lower(50000, seed=51)
+    Xt, B = synth.make_rhs(L, seed=51, nrhs=24)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, 512, "L", 1)
+    dB = _dev(B)
+    ref = _dev(np.zeros_like(B))
+    S.solve_batch(dB, ref, mode=mode, tol=1e-12, maxit=8)
+    need = S.workspace_bytes(mode, True)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda:0")
+    S.set_workspace(ws)
+    dX = _dev(np.zeros_like(B))
+    it, r = S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8)
+    assert r <= 1e-12
+    assert np.array_equal(dX.cpu().numpy(), ref.cpu().numpy())
+    S.set_workspace(ws[: need // 2])
+    with pytest.raises(spk.SpkError):
+        S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8)
+    S.set_workspace(None)
+    S.solve_batch(dB, dX, mode=mode, tol=1e-12, maxit=8)
+    assert rel_err(dX.cpu().numpy()[0], Xt[0]) <= 1e-12
