@@ -52,6 +52,23 @@ def alg_bytes(m: int, nnz: int) -> int:
     return 12 * nnz + 4 * (m + 1) + 16 * m
 
 
+def max_over_ranks(x: float, device, world: int) -> float:
+    """The largest of every rank's x (one all-reduce; the timing rule of the
+    multi-GPU replicas: the job takes as long as its slowest rank)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(ms_max: float, world: int) -> float:
+    """Whole-job solves/s of `world` replicas that each solve once per step."""
+    return world * 1e3 / ms_max
+
+
 def batched_bytes(m: int, nnz: int, k: int, mode: int, iters: int) -> int:
     """Algorithmic bytes of one batch of k right-hand sides: FP64 solve
     12 nnz + 4 (m+1) + 16 k m; FP32 solve 8 nnz + 4 (m+1) + 16 k m, plus per
@@ -307,11 +324,8 @@ def run_ours(args):
     launches = S.scalar("launches") - launches0
     S.check()
     ms = e0.elapsed_time(e1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * 1e3 / ms_max
+    ms_max = max_over_ranks(ms, dev, world)
+    value = replicas_value(ms_max, world)
 
     # dominant kernel: the segment-solver launches (phases 1 and 3+4), event-timed per phase
     S.set_profiling(True)
@@ -350,10 +364,7 @@ def run_ours(args):
     for _ in range(n_e2e):
         spk.spike_pstrsv_solve("L", m, bn, xn, args.P)
     e2e_s = (time.perf_counter() - t0) / n_e2e
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world / float(te.item())
+    e2e_value = world / max_over_ranks(e2e_s, dev, world)
 
     # batched forms of the same system (32 right-hand sides per batch)
     nb_steps = max(10, args.steps // 8)
