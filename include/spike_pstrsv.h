@@ -266,11 +266,13 @@ int spk_server_submit(spk_server *srv, int id, int nrhs, const double *b, double
  * batch's right-hand-side count. */
 int spk_server_wait(spk_server *srv, long long ticket, double *latency_s, double *resid, int *iters,
                     int *batch_rhs);
-/* out[0..10]: resident bytes, staging bytes, resident systems, evictions,
+/* out[0..14]: resident bytes, staging bytes, resident systems, evictions,
  * preprocessings, batches, right-hand sides batched, requests completed, budget,
  * batches retried after releasing idle systems when device memory ran out,
  * batches solved again in FP64 because their scaled residual was above 1e-12
- * (requests still above it fail with SPK_ERR_INPUT). */
+ * (requests still above it fail with SPK_ERR_INPUT), and microseconds spent
+ * (summed over the workers) in host staging in, the solves with their device
+ * copies, host staging out and preprocessing. */
 int spk_server_stats(spk_server *srv, long long *out, int count);
 
 /* The system used by the Part-1 entry points (NULL before the first preproc). */

@@ -25,6 +25,7 @@
 //   scaled residual of its batch.
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -91,6 +92,9 @@ struct spk_server {
     long long next_ticket = 1, clock = 0;
     long long evictions = 0, preprocs = 0, batches = 0, batched_rhs = 0, completed = 0, nomem_retries = 0;
     long long rechecks = 0;
+    // microseconds spent, summed over the workers: host staging in, solve (with
+    // the device copies), host staging out, preprocessing
+    std::atomic<long long> us_in{0}, us_solve{0}, us_out{0}, us_pre{0};
     int device = 0;
     bool stop = false;
 };
@@ -168,6 +172,27 @@ int ensure_slot_capacity(spk_server *S, Slot *sl, size_t doubles) {
     return SPK_OK;
 }
 
+// Host copy split across threads when large (the staging of a batch's right-hand
+// sides and solutions runs at host memory bandwidth, not one core's).
+void par_memcpy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kSplit = 8u << 20;
+    constexpr int kThreads = 4;
+    if (bytes < kSplit) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes / kThreads + 63) & ~size_t(63);
+    std::thread th[kThreads - 1];
+    for (int t = 1; t < kThreads; t++) {
+        const size_t off = part * t;
+        if (off >= bytes) break;
+        th[t - 1] = std::thread([=] { memcpy((char *)dst + off, (const char *)src + off, std::min(part, bytes - off)); });
+    }
+    memcpy(dst, src, std::min(part, bytes));
+    for (auto &t : th)
+        if (t.joinable()) t.join();
+}
+
 // The slot's workspace, grown to what a batch on this system needs.
 int ensure_slot_workspace(spk_server *S, Slot *sl, spk_system *sys) {
     const long long need = spk_workspace_bytes(sys, SPK_MODE_FP32_IR, 1);
@@ -190,11 +215,13 @@ int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch,
     SPK_TRY(ensure_slot_capacity(S, sl, (size_t)k * n));
     SPK_TRY(ensure_slot_workspace(S, sl, M->sys));
     SPK_TRY(spk_set_workspace(M->sys, sl->ws.p, (long long)sl->ws.n));
+    const double t0 = wall_s();
     int c = 0;
     for (Request *r : batch) {
-        memcpy(sl->hB + (size_t)c * n, r->b, sizeof(double) * r->nrhs * n);
+        par_memcpy(sl->hB + (size_t)c * n, r->b, sizeof(double) * r->nrhs * n);
         c += r->nrhs;
     }
+    const double t1 = wall_s();
     SPK_CUDA(cudaMemcpyAsync(sl->dB, sl->hB, sizeof(double) * k * n, cudaMemcpyHostToDevice, sl->st));
     // FP32 + refinement iterates to scaled residual <= 1e-12; every batch reports
     // its scaled residual (the caller checks it)
@@ -206,11 +233,16 @@ int run_batch(spk_server *S, Slot *sl, Matrix *M, std::vector<Request *> &batch,
     if (rc != SPK_OK) return rc;
     SPK_CUDA(e);
     SPK_TRY(spk_check(M->sys));
+    const double t2 = wall_s();
     c = 0;
     for (Request *r : batch) {
-        memcpy(r->x, sl->hX + (size_t)c * n, sizeof(double) * r->nrhs * n);
+        par_memcpy(r->x, sl->hX + (size_t)c * n, sizeof(double) * r->nrhs * n);
         c += r->nrhs;
     }
+    const double t3 = wall_s();
+    S->us_in += (long long)((t1 - t0) * 1e6);
+    S->us_solve += (long long)((t2 - t1) * 1e6);
+    S->us_out += (long long)((t3 - t2) * 1e6);
     return SPK_OK;
 }
 
@@ -260,11 +292,13 @@ void worker(spk_server *S, Slot *sl) {
                 S->cv_done.wait(lk);
             }
             lk.unlock();
+            const double tp = wall_s();
             spk_system *sys = nullptr;
             status = spk_create(&sys);
             if (status == SPK_OK)
                 status = spk_preproc(sys, M->a.data(), M->ia.data(), M->ja.data(), M->n, M->nparts, M->uplo, 1,
                                      nullptr, nullptr);
+            S->us_pre += (long long)((wall_s() - tp) * 1e6);
             lk.lock();
             if (status == SPK_OK) {
                 M->sys = sys;
@@ -477,9 +511,10 @@ int spk_server_stats(spk_server *S, long long *out, int count) {
     std::lock_guard<std::mutex> g(S->mu);
     long long nres = 0;
     for (auto &kv : S->mats) nres += kv.second->sys != nullptr;
-    const long long v[11] = {S->resident, S->workspace, nres, S->evictions, S->preprocs,     S->batches,
-                             S->batched_rhs, S->completed, S->budget,   S->nomem_retries, S->rechecks};
-    for (int i = 0; i < count && i < 11; i++) out[i] = v[i];
+    const long long v[15] = {S->resident,      S->workspace,    nres,           S->evictions,     S->preprocs,
+                             S->batches,       S->batched_rhs,  S->completed,   S->budget,        S->nomem_retries,
+                             S->rechecks,      S->us_in.load(), S->us_solve.load(), S->us_out.load(), S->us_pre.load()};
+    for (int i = 0; i < count && i < 15; i++) out[i] = v[i];
     return SPK_OK;
 }
 

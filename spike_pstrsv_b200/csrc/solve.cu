@@ -504,23 +504,7 @@ __device__ bool tile_range(const TileArgs &A, TileSmemK<K, T> &S, unsigned &phas
             const int *cs = S.c[slot];
             const T *vg = evg + p_lo;
             const int *cg = A.ell_col + p_lo;
-            for (int k0 = 0; k0 < width; k0 += CH) {
-                int cr[CH];
-                T vr[CH];
-#pragma unroll
-                for (int u = 0; u < CH; u++) {
-                    const int k = k0 + u;
-                    if (k < nst) {
-                        cr[u] = cs[k * 32 + lane];
-                        vr[u] = vs[k * 32 + lane];
-                    } else if (k < width) {
-                        cr[u] = cg[k * 32 + lane];
-                        vr[u] = vg[k * 32 + lane];
-                    } else {
-                        cr[u] = row;  // no-op slot: zero into the row's own (diagonal) position
-                        vr[u] = T(0);
-                    }
-                }
+            auto chunk = [&](const int (&cr)[CH], const T (&vr)[CH]) {
                 int ci[CH];
                 T rr[CH], wr[CH][K];
 #pragma unroll
@@ -539,6 +523,31 @@ __device__ bool tile_range(const TileArgs &A, TileSmemK<K, T> &S, unsigned &phas
                         pacc[k][u % NP] = in_win ? fma(vr[u], wr[u][k], pacc[k][u % NP]) : pacc[k][u % NP];
                     slow = slow || (ci[u] == 32 && !in_win && (FULL || cr[u] < hi_ext));
                 }
+            };
+            // staged slots (the common case: the tile's width fits the stage); a
+            // loop of its own, so that its loads are shared-memory loads only
+            for (int k0 = 0; k0 < nst; k0 += CH) {
+                int cr[CH];
+                T vr[CH];
+#pragma unroll
+                for (int u = 0; u < CH; u++) {
+                    const int k = k0 + u;
+                    cr[u] = k < nst ? cs[k * 32 + lane] : row;  // no-op slot: zero into the row's own position
+                    vr[u] = k < nst ? vs[k * 32 + lane] : T(0);
+                }
+                chunk(cr, vr);
+            }
+            // slots beyond the stage, from global memory
+            for (int k0 = nst; k0 < width; k0 += CH) {
+                int cr[CH];
+                T vr[CH];
+#pragma unroll
+                for (int u = 0; u < CH; u++) {
+                    const int k = k0 + u;
+                    cr[u] = k < width ? cg[k * 32 + lane] : row;
+                    vr[u] = k < width ? vg[k * 32 + lane] : T(0);
+                }
+                chunk(cr, vr);
             }
         }
         if (__any_sync(FULLMASK, slow) && act) {
