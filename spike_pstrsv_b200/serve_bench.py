@@ -18,7 +18,7 @@ the server's batching and residency counters.  The comparison is the plain
 FP64 path, one solve per call with host arrays (spk_solve), on the same request
 mix: solves/s = right-hand sides / the sum of their per-matrix solve times.
 
-    python -m spike_pstrsv_b200.serve_bench [--full] [--rates 50,150,500,2000]
+    python -m spike_pstrsv_b200.serve_bench [--full] [--rates 50,150,500,2000] [--mode fp32ir|fp64]
 """
 from __future__ import annotations
 
@@ -193,8 +193,10 @@ def main():
     ap.add_argument("--rates", default="50,150,500,2000")
     ap.add_argument("--requests", type=int, default=None)
     ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--mode", default="fp32ir", choices=["fp32ir", "fp64"])
     args = ap.parse_args()
-    out = run(args.full, [float(r) for r in args.rates.split(",")], args.requests, args.slots)
+    mode = serve.MODE_FP32_IR if args.mode == "fp32ir" else serve.MODE_FP64
+    out = run(args.full, [float(r) for r in args.rates.split(",")], args.requests, args.slots, mode=mode)
     print(json.dumps(out))
 
 
