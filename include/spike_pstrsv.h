@@ -159,6 +159,20 @@ enum { SPK_MODE_FP64 = 0, SPK_MODE_FP32_IR = 1 };
 int spk_solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx, int mode,
                     double tol, int maxit, void *stream, int *iters, double *resid);
 
+/* MatrixMarket coordinate file (real, integer or double values) into a 0-based
+ * CSR (src/misc.h:35, src/misc.c:109-245): uplo 'U' keeps row <= column, 'L'
+ * row >= column, 'N' all entries; symm 'Y' mirrors the off-diagonal entries of a
+ * symmetric file ('S' and 'N' read the entries as they are); entries sorted by
+ * (row, column); *numRows is the column count.  Host code, no GPU.  The arrays
+ * come from posix_memalign: release them with free() (or spk_mtx_free), not
+ * mkl_free.  On failure the pointers are NULL and the reason is printed. */
+void matrixMarketToCSR(const char *filename, double **a, MKL_INT **ia, MKL_INT **ja, int *numRows, const char uplo,
+                       const char symm);
+/* The same with a status code (SPK_ERR_INPUT for unreadable, malformed or pattern
+ * files) and the entry count. */
+int spk_mtx_read(const char *path, char uplo, char symm, double **a, int **ia, int **ja, int *n, int *nnz);
+void spk_mtx_free(double *a, int *ia, int *ja);
+
 /* Lend the system device memory for the batched solves' work columns (no
  * reference counterpart): with a workspace set, spk_solve_batch carves its
  * work, residual and correction columns (32 x n FP64 each, as needed) from it

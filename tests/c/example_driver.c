@@ -1,7 +1,8 @@
 /* C caller of the drop-in ABI in the call pattern of the reference's
  * example_usage.c (single call, then preprocess once + solve) and of its
  * profiler (timed variants, PSTRSV_VERBOSE).  Builds the lower triangle of the
- * 5-point Poisson matrix on an N x N grid, b = L x_real with the reference's
+ * 5-point Poisson matrix on an N x N grid (or, with a third argument, reads the
+ * lower triangle of a MatrixMarket file), b = L x_real with the reference's
  * known-answer x_real = (rand()%71)+1 + (i%1000)/10 (example_usage.c:81-85), and
  * prints the 2-norm error of each solve.  Exit status 0 when every error is
  * below the reference's 1e-4 acceptance threshold. */
@@ -21,18 +22,28 @@ static double err2(const double *x, const double *xr, int m) {
 int main(int argc, char **argv) {
     const int N = argc > 1 ? atoi(argv[1]) : 64;
     const int P = argc > 2 ? atoi(argv[2]) : 4;
-    const int m = N * N;
-    MKL_INT *ia = malloc(sizeof(MKL_INT) * (m + 1));
-    MKL_INT *ja = malloc(sizeof(MKL_INT) * 3 * m);
-    double *a = malloc(sizeof(double) * 3 * m);
-    int q = 0;
-    for (int i = 0; i < m; i++) {
-        ia[i] = q;
-        if (i >= N) { ja[q] = i - N; a[q++] = -1.0; }
-        if (i % N) { ja[q] = i - 1; a[q++] = -1.0; }
-        ja[q] = i; a[q++] = 4.0;
+    int m = N * N;
+    MKL_INT *ia, *ja;
+    double *a;
+    if (argc > 3) {
+        /* the profiler's way in (runtime_analysis.c:290-292): a MatrixMarket file,
+         * lower triangle */
+        matrixMarketToCSR(argv[3], &a, &ia, &ja, &m, 'L', 'N');
+        if (!a) return 2;
+        printf("read %s: %d rows, %d entries\n", argv[3], m, ia[m]);
+    } else {
+        ia = malloc(sizeof(MKL_INT) * (m + 1));
+        ja = malloc(sizeof(MKL_INT) * 3 * m);
+        a = malloc(sizeof(double) * 3 * m);
+        int q = 0;
+        for (int i = 0; i < m; i++) {
+            ia[i] = q;
+            if (i >= N) { ja[q] = i - N; a[q++] = -1.0; }
+            if (i % N) { ja[q] = i - 1; a[q++] = -1.0; }
+            ja[q] = i; a[q++] = 4.0;
+        }
+        ia[m] = q;
     }
-    ia[m] = q;
     double *xr = malloc(sizeof(double) * m), *b = calloc(m, sizeof(double));
     double *b2 = malloc(sizeof(double) * m), *x = calloc(m, sizeof(double));
     for (int i = 0; i < m; i++) xr[i] = ((rand() % 71) + 1) + ((double)(i % 1000) / 10.0);

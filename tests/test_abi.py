@@ -74,3 +74,16 @@ def test_c_caller_runs(tmp_path):
     out = subprocess.run([exe, "96", "6"], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "Reduced system size" in out.stdout  # logPSTRSV3 text format
+
+
+@pytest.mark.gpu
+def test_c_caller_runs_on_a_matrix_market_file(tmp_path):
+    """The profiler's way in: matrixMarketToCSR then the drop-in solve."""
+    from spike_pstrsv_b200 import mtx, synth
+    L = synth.poisson2d_lower(64)
+    path = str(tmp_path / "poisson64.mtx")
+    mtx.write(path, L)
+    exe = build_c_driver(tmp_path)
+    out = subprocess.run([exe, "64", "4", path], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert f"read {path}: {L.m} rows, {L.nnz} entries" in out.stdout
