@@ -265,8 +265,9 @@ int spk_group_destroy(spk_group *g);
  * while other batches run join the next batch and batches of different
  * matrices overlap on the device.  Requests take host arrays (column-major,
  * leading dimension n) that must stay valid until spk_server_wait returns.
- * SPK_MODE_FP32_IR requests iterate to scaled residual <= 1e-12; every batch's
- * scaled residual is checked against 1e-12. */
+ * SPK_MODE_FP32_IR batches take one FP64-residual correction step; every batch's
+ * scaled residual is checked against 1e-12 (a batch above it is solved again in
+ * FP64). */
 typedef struct spk_server spk_server;
 int spk_server_create(spk_server **out, long long hbm_budget_bytes, int nslots);
 int spk_server_destroy(spk_server *srv);
