@@ -579,7 +579,30 @@ __device__ bool tile_range(const TileArgs &A, TileSmemK<K, T> &S, unsigned &phas
         // in-tile triangle over the active rows (bottom-up); a lane's accumulators
         // are final after its own step
         const int i_hi = a1 - 1 - row0, i_lo = a0 - row0;
-        if (i_hi == 31 && i_lo == 0) {
+        if (i_hi == 31 && i_lo == 0 && K == 1) {
+            // blocks of four rows (i, i-1, i-2, i-3): the four accumulators are
+            // broadcast together, every lane resolves the block's four unknowns from
+            // the in-block coefficients (uniform loads) and applies all four columns;
+            // a lane's own coefficients for columns at or below its row are zero, so
+            // lanes inside the block come out with their final values too
+#pragma unroll
+            for (int i = 31; i >= 3; i -= 4) {
+                const T c0 = S.coef[i][lane], c1 = S.coef[i - 1][lane];
+                const T c2 = S.coef[i - 2][lane], c3 = S.coef[i - 3][lane];
+                const T u10 = S.coef[i][i - 1];
+                const T u20 = S.coef[i][i - 2], u21 = S.coef[i - 1][i - 2];
+                const T u30 = S.coef[i][i - 3], u31 = S.coef[i - 1][i - 3], u32 = S.coef[i - 2][i - 3];
+                const T b0 = __shfl_sync(FULLMASK, acc[0], i), b1 = __shfl_sync(FULLMASK, acc[0], i - 1);
+                const T b2 = __shfl_sync(FULLMASK, acc[0], i - 2), b3 = __shfl_sync(FULLMASK, acc[0], i - 3);
+                const T a1 = fma(-u10, b0, b1);
+                const T a2 = fma(-u21, a1, fma(-u20, b0, b2));
+                const T a3 = fma(-u32, a2, fma(-u31, a1, fma(-u30, b0, b3)));
+                T t = fma(-c0, b0, acc[0]);
+                t = fma(-c1, a1, t);
+                t = fma(-c2, a2, t);
+                acc[0] = fma(-c3, a3, t);
+            }
+        } else if (i_hi == 31 && i_lo == 0) {
 #pragma unroll
             for (int i = 31; i >= 0; i--) {
                 const T ci = S.coef[i][lane];
