@@ -42,10 +42,20 @@ def build(ref: bool | None = None) -> None:
     import subprocess
 
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    src = ref_source_dir()
     if ref is None:
-        ref = os.path.isdir("/root/reference/src")
+        ref = os.path.isdir(src)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "SPK_REF_SRC=" + src], check=True)
+
+
+def ref_source_dir() -> str:
+    """The reference tree's ``src/`` folder: ``$SPK_REF_SRC`` when set, else a
+    checkout named ``reference`` beside the repository (the Makefile's default)."""
+    env = os.environ.get("SPK_REF_SRC")
+    if env:
+        return os.path.abspath(env)
+    return os.path.abspath(os.path.join(HERE, "..", "..", "reference", "src"))
 
 
 def _i32(x):
@@ -155,6 +165,11 @@ class Reference:
     @classmethod
     def available(cls) -> bool:
         return os.path.exists(REF_SO)
+
+    @classmethod
+    def missing_reason(cls) -> str:
+        return (f"reference checker {REF_SO} not built (make -C oracle ref, with the reference "
+                f"sources at {ref_source_dir()} or SPK_REF_SRC)")
 
     @classmethod
     def lib(cls):

@@ -47,7 +47,7 @@ def _dense(A):
 
 def _reference_read(path, uplo, symm):
     if not oracle.Reference.available():
-        pytest.skip("the reference build (oracle/_ref) is not present")
+        pytest.skip(oracle.Reference.missing_reason())
     L = oracle.Reference.lib()
     dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
     f = L.matrixMarketToCSR

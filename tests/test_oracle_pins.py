@@ -88,7 +88,7 @@ def test_oracle_matches_golden_digest(name):
     assert rel_err(x, x_true) <= 1e-12
 
 
-needs_ref = pytest.mark.skipif(not oracle.Reference.available(), reason="reference checker not built")
+needs_ref = pytest.mark.skipif(not oracle.Reference.available(), reason=oracle.Reference.missing_reason())
 
 
 @needs_ref
