@@ -233,6 +233,13 @@ int spk_debug_array(const spk_system *s, const char *name, void *dst, long long 
                     long long *count, char *type);
 long long spk_debug_scalar(const spk_system *s, const char *name);
 
+/* Test hook (no reference counterpart): spk_debug_set(s, "fail_waits", 1) makes
+ * every solve kernel of s report a failed bounded wait at entry, before it
+ * issues any copy, until the failure has been reported once (SPK_ERR_TIMEOUT
+ * from the synchronous solve or spk_check); the next solve then runs normally.
+ * It exercises the error path of the bounded waits without a real hang. */
+int spk_debug_set(spk_system *s, const char *name, long long value);
+
 /* Many systems solved by one captured launch sequence (no reference
  * counterpart).  count preprocessed systems (sliced-ELL layout), system i with
  * nrhs[i] right-hand sides in device array B[i] (column-major, leading dimension

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspike_pstrsv_b200.so")
 
-SOURCES = ["preproc.cu", "solve.cu", "capi.cu", "server.cu", "mtx.cu"]
+SOURCES = ["preproc.cu", "solve.cu", "chain.cu", "capi.cu", "server.cu", "mtx.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O2",
          "-Xptxas", "-warn-spills"]

@@ -57,6 +57,7 @@ def lib() -> ctypes.CDLL:
                                       ctypes.POINTER(ctypes.c_longlong), ctypes.c_char_p]
         L.spk_debug_scalar.restype = ctypes.c_longlong
         L.spk_debug_scalar.argtypes = [vp, ctypes.c_char_p]
+        L.spk_debug_set.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
         L.spk_legacy_system.restype = vp
         L.spk_set_truncation.argtypes = [vp, d]
         L.spk_check.argtypes = [vp]
@@ -298,6 +299,12 @@ class System:
 
     def scalar(self, name: str) -> int:
         return int(lib().spk_debug_scalar(self.h, name.encode()))
+
+    def debug_set(self, name: str, value: int) -> "System":
+        """Test hooks (spk_debug_set): "fail_waits" makes the solve kernels report a
+        failed bounded wait until the failure has been reported once."""
+        _check(lib().spk_debug_set(self.h, name.encode(), int(value)))
+        return self
 
     def structure(self) -> dict:
         from_names = [

@@ -104,6 +104,9 @@ void destroy_system(spk_system *s) {
         for (auto &e : set)
             if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    for (cudaEvent_t e : s->pipe_ev) cudaEventDestroy(e);
+    if (s->st_in) cudaStreamDestroy(s->st_in);
+    if (s->st_out) cudaStreamDestroy(s->st_out);
     delete s;
 }
 
@@ -204,18 +207,25 @@ void legacy_solve(char uplo, int m, double *b, double *x, int nthreads, bool tim
         clock_gettime(CLOCK_MONOTONIC, &ts);
         t0 = ts.tv_sec + 1e-9 * ts.tv_nsec;
     }
+    if (!bd && g_b.n < (size_t)m && g_b.alloc(m) != SPK_OK) { report("solve"); return; }
+    if (!xd) {
+        if (g_x.n < (size_t)m && g_x.alloc(m) != SPK_OK) { report("solve"); return; }
+        dx = g_x.p;
+    }
+    if (!bd && !xd && !timed && !SPK_CLOBBER_B && s->chain_ok) {
+        // host arrays: copies overlapped with the solve, chunk by chunk
+        int rc = chain_solve_host(s, b, x, g_b.p, g_x.p);
+        if (rc == SPK_OK) rc = check_device_error(s);
+        if (rc != SPK_OK) report("solve");
+        return;
+    }
     if (!bd) {
-        if (g_b.n < (size_t)m && g_b.alloc(m) != SPK_OK) { report("solve"); return; }
         if (cudaMemcpyAsync(g_b.p, b, sizeof(double) * m, cudaMemcpyHostToDevice, st) != cudaSuccess) {
             set_error(SPK_ERR_CUDA, "copy of b to the device failed");
             report("solve");
             return;
         }
         db = g_b.p;
-    }
-    if (!xd) {
-        if (g_x.n < (size_t)m && g_x.alloc(m) != SPK_OK) { report("solve"); return; }
-        dx = g_x.p;
     }
     int rc = solve(s, db, dx, st, timed ? ph : nullptr);
     if (rc == SPK_OK && SPK_CLOBBER_B) {
@@ -354,13 +364,17 @@ int spk_solve(spk_system *s, const double *b, double *x) {
     double *dx = x;
     if (!bd) {
         if (s->stage_b.n < (size_t)n) SPK_TRY(s->stage_b.alloc(n));
-        SPK_CUDA(cudaMemcpyAsync(s->stage_b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
         db = s->stage_b.p;
     }
     if (!xd) {
         if (s->stage_x.n < (size_t)n) SPK_TRY(s->stage_x.alloc(n));
         dx = s->stage_x.p;
     }
+    if (!bd && !xd && s->chain_ok) {
+        SPK_TRY(chain_solve_host(s, b, x, s->stage_b.p, s->stage_x.p));
+        return check_device_error(s);
+    }
+    if (!bd) SPK_CUDA(cudaMemcpyAsync(s->stage_b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
     SPK_TRY(solve(s, db, dx, s->stream, nullptr));
     if (!xd) SPK_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
     SPK_CUDA(cudaStreamSynchronize(s->stream));
@@ -481,7 +495,19 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "launches")) return s->launches;
     if (!strcmp(name, "ell")) return s->ell_ok;
     if (!strcmp(name, "ell_entries")) return s->ell_entries;
-    if (!strcmp(name, "launches_per_solve")) return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
+    if (!strcmp(name, "launches_per_solve")) {
+        if (s->chain_ok) return (s->nctasks1 ? 1 : 0) + (s->nctasks4 ? 1 : 0);
+        return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
+    }
+    if (!strcmp(name, "chain")) return s->chain_ok;
+    if (!strcmp(name, "chains")) return s->ch_count;
+    if (!strcmp(name, "chain_rows")) return s->ch_len;
+    if (!strcmp(name, "chain_width")) return s->ch_width;
+    if (!strcmp(name, "chain_reach")) return s->ch_reach;
+    if (!strcmp(name, "chain_rows_phase1")) return s->ch_rows1;
+    if (!strcmp(name, "chain_rows_phase4")) return s->ch_rows4;
+    if (!strcmp(name, "chain_tasks_phase4")) return s->nctasks4;
+    if (!strcmp(name, "chain_bytes")) return (long long)(s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes());
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
     if (!strcmp(name, "kept_reduced_rows")) return s->nkept;
     if (!strcmp(name, "reduced_levels")) return s->nlvl;
@@ -494,9 +520,23 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
         b += s->ell_valf.bytes() + s->rdiagf.bytes() + s->diag.bytes() + s->rbuf.bytes() + s->dbuf.bytes() + s->work.bytes();
         b += s->stage_b.bytes() + s->stage_x.bytes();
+        b += s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes() + s->d_ctasks1.bytes() + s->d_ctasks4.bytes();
         return b;
     }
     return -1;
+}
+
+int spk_debug_set(spk_system *s, const char *name, long long value) {
+    if (!s || !name) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!strcmp(name, "fail_waits")) {
+        s->dbg_fail_waits = value != 0;
+        return SPK_OK;
+    }
+    set_error(SPK_ERR_ARG, "unknown debug setting '%s'", name);
+    return SPK_ERR_ARG;
 }
 
 int spk_debug_array(const spk_system *s, const char *name, void *dst, long long cap, long long *count,

@@ -1,0 +1,592 @@
+// Chain solver: the default one-right-hand-side FP64 solve of
+// spike_pstrsv_solve (src/spike_pstrsv.c:149-239) when spike truncation is on.
+//
+// Decomposition.  The rows of U are cut into chains [a, q) of a few thousand
+// rows, aligned to 32-row tiles and independent of the caller's partition count
+// (the partitions still define every piece of reference state; only the solve's
+// task decomposition differs).  For a chain, x - y = -S x_c exactly, where y is
+// the chain-local solution (columns >= q taken as zero), x_c the true values of
+// the columns >= q and S = D_chain^{-1} R_chain the chain's spike: the same
+// identity the reference's phases 1-4 rest on (src/spike_pstrsv.c:194-229), with
+// the chain in the role of a partition.  Preprocessing computes every chain's
+// spike exactly (k_chain_spike) and finds f, the first row from the top whose
+// spike row has an absolute sum above tau (2^-60 by default, below FP64
+// resolution relative to ||x||_inf).  Rows [a, f) of y are final.
+//
+//   phase 1   every chain solves [a, q) with zero coupling and stores rows [a, f)
+//   phase 4   every chain with f < q re-solves [f, q), reading the columns >= q
+//             from x (rows that phase 1 of the chain below stored)
+//
+// Valid when every chain but the top one keeps its first `reach` rows (f >= a +
+// reach, reach = the widest column distance): then phase 4 only reads final
+// values.  Preprocessing doubles the chain length until that holds, and falls
+// back to the partition-based solve otherwise.
+//
+// Kernel.  One warp per task, lane = row of a 32-row tile, tiles bottom-up.  The
+// matrix is stored for this solver as a sliced ELL of ROW-SCALED off-diagonals
+// a(r,c)/a(r,r) (so x_r = b_r/a(r,r) - sum v'(r,c) x_c) with 8-bit column
+// offsets c - r, per tile slot-pair-major (values: one 16-byte load per lane
+// per two slots; offsets: one 4-byte load per lane per four slots).  Each tile
+// is loaded straight into registers two tiles ahead, so shared memory carries
+// only the solved-row window (gathers of far columns) and a per-lane column of
+// in-tile coefficients: coef[i][lane] = v'(row0+lane, row0+i) is written and
+// read by its own lane only, so the in-tile triangle needs no barrier beyond
+// the warp shuffles that broadcast each solved row.
+//
+// Memory per solve (banded workload, 16 off-diagonals per row): 16 x 9 B of
+// matrix + 8 B 1/diagonal + 8 B b + 8 B x per row in phase 1, the same per
+// re-solved row in phase 4.  No scratch vector: phase 1 writes final rows
+// straight into x.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "spk_internal.cuh"
+
+namespace spk {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+inline int nblocks(long long n, int bs = 256) { return (int)((n + bs - 1) / bs); }
+
+// ---- layout construction -----------------------------------------------------------
+
+// Per 32-row tile: the widest row (off-diagonal count) and, over all rows, the
+// widest column distance (last column - row; columns are sorted).
+__global__ void k_chain_scan(int n, const int *__restrict__ ia, const int *__restrict__ ja, int *__restrict__ width,
+                             int *__restrict__ reach) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    int len = 0, dist = 0;
+    if (r < n) {
+        const int b = ia[r], e = ia[r + 1];
+        len = e - b - 1;
+        dist = len > 0 ? ja[e - 1] - r : 0;
+    }
+    int w = len, d = dist;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        w = max(w, __shfl_xor_sync(kFull, w, o));
+        d = max(d, __shfl_xor_sync(kFull, d, o));
+    }
+    if ((threadIdx.x & 31) == 0 && (r >> 5) < (n + 31) / 32) {
+        width[r >> 5] = w;
+        atomicMax(reach, d);
+    }
+}
+
+// Slots of tile j = rows 32j..32j+31: slot k of lane l holds value
+// val[ptr_j + (k>>1)*64 + 2l + (k&1)] and offset byte off[ptr_j + (k>>2)*128 +
+// 4l + (k&3)]; padding: value 0, offset 0 (column = the row itself).
+__global__ void k_chain_fill(int n, int ntiles, const int *__restrict__ ia, const int *__restrict__ ja,
+                             const double *__restrict__ a, const int *__restrict__ ptr, double *__restrict__ val,
+                             unsigned char *__restrict__ off) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = r >> 5, l = r & 31;
+    if (j >= ntiles) return;
+    const int w = (ptr[j + 1] - ptr[j]) >> 5;
+    const long long base = ptr[j];
+    int b = 0, len = 0;
+    double rd = 0.0;
+    if (r < n) {
+        b = ia[r];
+        len = ia[r + 1] - b - 1;
+        rd = 1.0 / a[b];
+    }
+    for (int k = 0; k < w; k++) {
+        const long long vo = base + (k >> 1) * 64 + 2 * l + (k & 1);
+        const long long oo = base + (k >> 2) * 128 + 4 * l + (k & 3);
+        if (k < len) {
+            val[vo] = a[b + 1 + k] * rd;
+            off[oo] = (unsigned char)(ja[b + 1 + k] - r);
+        } else {
+            val[vo] = 0.0;
+            off[oo] = 0;
+        }
+    }
+}
+
+// ---- spikes of the chains -------------------------------------------------------------
+//
+// One warp per chain [a, q); lane owns spike columns lane + 32 cc (cc < C), i.e.
+// the unit responses to x at columns q + lane + 32 cc.  A ring of reach + 1 rows
+// in shared memory ([slot][32 C]) holds the spike rows the recurrence still
+// reads; rows [q, q + reach) start as unit vectors, and every row r < q is
+// X_r = -sum_k v'(r, r + off_k) X_{r + off_k}.  Each lane reads only its own
+// columns, so the ring needs no barrier.  f = the smallest row whose absolute
+// row sum exceeds tau (q when none).
+
+struct SpikeArgs {
+    const int2 *chains;  // [a, q)
+    int nchains;
+    const double *val;
+    const unsigned *off;  // offset bytes as 32-bit words
+    const int *ptr;
+    int reach;
+    double tau;
+    int *first;
+};
+
+template <int C>
+__global__ void __launch_bounds__(32) k_chain_spike(SpikeArgs A) {
+    extern __shared__ double ring[];  // [(reach + 1) * 32 * C]
+    const int lane = threadIdx.x;
+    const int2 ch = A.chains[blockIdx.x];
+    const int a = ch.x, q = ch.y;
+    const int R = A.reach + 1;
+    // slot(q - 1) = 0, slot(q + j) = j + 1
+    for (int s = 0; s < R; s++) {
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) {
+            const int col = lane + 32 * cc;
+            ring[s * 32 * C + col] = (s >= 1 && col == s - 1) ? 1.0 : 0.0;
+        }
+    }
+    int first = q;
+    int sr = 0;  // slot of the current row
+    for (int r = q - 1; r >= a; r--) {
+        const int j = r >> 5, l = r & 31;
+        const int p0 = A.ptr[j];
+        const int w = (A.ptr[j + 1] - p0) >> 5;
+        double acc[C][2];
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) acc[cc][0] = acc[cc][1] = 0.0;
+        for (int k0 = 0; k0 < w; k0 += 4) {
+            const unsigned ow = __ldg(A.off + ((p0 + (k0 >> 2) * 128) >> 2) + l);
+            const double2 va = __ldg((const double2 *)(A.val + p0 + (k0 >> 1) * 64) + l);
+            const double2 vb = __ldg((const double2 *)(A.val + p0 + ((k0 >> 1) + 1) * 64) + l);
+            const double v4[4] = {va.x, va.y, vb.x, vb.y};
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int o = (ow >> (8 * u)) & 0xff;
+                int cs = sr + o;
+                cs -= cs >= R ? R : 0;
+#pragma unroll
+                for (int cc = 0; cc < C; cc++)
+                    acc[cc][u & 1] = fma(-v4[u], ring[cs * 32 * C + lane + 32 * cc], acc[cc][u & 1]);
+            }
+        }
+        double s = 0.0;
+#pragma unroll
+        for (int cc = 0; cc < C; cc++) {
+            const double x = acc[cc][0] + acc[cc][1];
+            ring[sr * 32 * C + lane + 32 * cc] = x;
+            s += fabs(x);
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+        if (!(s <= A.tau)) first = r;  // NaN counts as significant
+        sr = sr == 0 ? R - 1 : sr - 1;
+    }
+    if (lane == 0) A.first[blockIdx.x] = first;
+}
+
+// ---- the solve kernel -----------------------------------------------------------------
+
+struct ChainArgs {
+    const ChainTask *tasks;
+    const double *val;
+    const unsigned *off;
+    const int *ptr;
+    const double *rd;   // 1 / diagonal, padded to whole tiles
+    int n;
+    const double *b;    // caller order
+    double *x;          // caller order
+    int rev;            // uplo 'L': caller row i is U row n-1-i
+    int mask;           // window rows - 1 (power of two >= reach + 32)
+    int *err;
+    int fail_entry;     // test hook: report a failed wait and return (spk_debug_set "fail_waits")
+};
+
+template <int W>
+struct TileRegs {
+    double2 v[W / 2];
+    unsigned o[W / 4];
+    double b, rd;
+    int w;  // slots of this tile (multiple of 4)
+};
+
+template <int W>
+__device__ __forceinline__ void load_tile(const ChainArgs &A, TileRegs<W> &R, int j, int p0, int p1, int lo, int hi,
+                                          int lane) {
+    R.w = (p1 - p0) >> 5;
+    const double2 *vp = (const double2 *)(A.val + p0) + lane;
+    const unsigned *op = A.off + (p0 >> 2) + lane;
+#pragma unroll
+    for (int k = 0; k < W / 2; k++)
+        if (2 * k < R.w) R.v[k] = __ldg(vp + 32 * k);
+#pragma unroll
+    for (int k = 0; k < W / 4; k++)
+        if (4 * k < R.w) R.o[k] = __ldg(op + 32 * k);
+    const int r = 32 * j + lane;
+    const bool act = r >= lo && r < hi;
+    R.b = act ? __ldg(A.b + (A.rev ? A.n - 1 - r : r)) : 0.0;
+    R.rd = act ? __ldg(A.rd + r) : 0.0;
+}
+
+template <int W>
+__device__ __forceinline__ void solve_tile(const ChainArgs &A, const TileRegs<W> &R, int j, const ChainTask &t,
+                                           double *coef, double *win, int lane) {
+    const int row0 = 32 * j, r = row0 + lane;
+    const bool act = r >= t.lo && r < t.hi;
+    double acc = R.b * R.rd;
+    double p[4] = {0.0, 0.0, 0.0, 0.0};
+    // far columns from the window, in-tile columns into the lane's coefficient column
+#pragma unroll
+    for (int k = 0; k < W; k++) {
+        if (4 * (k >> 2) < R.w) {
+            const int o = (R.o[k >> 2] >> (8 * (k & 3))) & 0xff;
+            const double v = (k & 1) ? R.v[k >> 1].y : R.v[k >> 1].x;
+            const int d = lane + o;
+            if (act) {
+                if (d < 32) coef[d * 32 + lane] = v;
+                else p[k & 3] = fma(v, win[(row0 + d) & A.mask], p[k & 3]);
+            }
+        }
+    }
+    acc -= (p[0] + p[1]) + (p[2] + p[3]);
+    // in-tile triangle, bottom-up: row i is final when its lane broadcasts it
+#pragma unroll
+    for (int i = 31; i >= 0; i--) {
+        const double xi = __shfl_sync(kFull, acc, i);
+        acc = fma(-coef[i * 32 + lane], xi, acc);
+    }
+    if (act) {
+        win[r & A.mask] = acc;
+        if (r >= t.st_lo && r < t.st_hi) A.x[A.rev ? A.n - 1 - r : r] = acc;
+        // leave the coefficient column zero for the next tile
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+            if (4 * (k >> 2) < R.w) {
+                const int d = lane + ((R.o[k >> 2] >> (8 * (k & 3))) & 0xff);
+                if (d < 32) coef[d * 32 + lane] = 0.0;
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// PRE: phase 4 (the window starts with x of rows [hi, hi + window)); else
+// phase 1 (it starts at zero: zero coupling beyond the chain).
+template <bool PRE, int W>
+__global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
+    constexpr int NS = W <= 16 ? 3 : 2;  // register stages: tiles in flight = NS - 1
+    extern __shared__ double sm[];
+    double *coef = sm;        // [32 columns][32 lanes]
+    double *win = sm + 1024;  // [mask + 1]
+    const int lane = threadIdx.x;
+    if (A.fail_entry) {
+        if (lane == 0) atomicExch(A.err, 1);
+        return;
+    }
+    const ChainTask t = A.tasks[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < 32; i++) coef[i * 32 + lane] = 0.0;
+    for (int k = lane; k <= A.mask; k += 32) {
+        const int r = t.hi + k;
+        double v = 0.0;
+        if (PRE && r < A.n) v = A.x[A.rev ? A.n - 1 - r : r];  // rows >= hi + reach are loaded, never read
+        win[r & A.mask] = v;
+    }
+    __syncwarp();
+    const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
+    // tile jj uses register stage (jt - jj) % NS; its pointers are loaded one
+    // iteration before its slots, its slots NS - 1 iterations before it is solved
+    TileRegs<W> R[NS];
+    int P0[NS], P1[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const int jj = jt - s;
+        if (jj >= jb) {
+            P0[s] = __ldg(A.ptr + jj);
+            P1[s] = __ldg(A.ptr + jj + 1);
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS - 1; s++)
+        if (jt - s >= jb) load_tile<W>(A, R[s], jt - s, P0[s], P1[s], t.lo, t.hi, lane);
+    for (int j0 = jt; j0 >= jb; j0 -= NS) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const int j = j0 - s;
+            if (j >= jb) {
+                const int sl = (s + NS - 1) % NS;  // stage of tile j - (NS - 1)
+                const int jl = j - (NS - 1);
+                if (jl >= jb) load_tile<W>(A, R[sl], jl, P0[sl], P1[sl], t.lo, t.hi, lane);
+                // pointers of tile j - NS into this tile's stage (its own are consumed)
+                const int jp = j - NS;
+                if (jp >= jb) {
+                    P0[s] = __ldg(A.ptr + jp);
+                    P1[s] = __ldg(A.ptr + jp + 1);
+                }
+                solve_tile<W>(A, R[s], j, t, coef, win, lane);
+            }
+        }
+    }
+}
+
+template <bool PRE>
+int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double *b, double *x, cudaStream_t st) {
+    if (ntasks <= 0) return SPK_OK;
+    ChainArgs A;
+    A.tasks = tasks;
+    A.val = s->ch_val.p;
+    A.off = (const unsigned *)s->ch_off.p;
+    A.ptr = s->ch_ptr.p;
+    A.rd = s->rdiag.p;
+    A.n = s->n;
+    A.b = b;
+    A.x = x;
+    A.rev = s->uplo == 'L';
+    A.mask = s->ch_win - 1;
+    A.err = s->d_err.p;
+    A.fail_entry = s->dbg_fail_waits > 0;
+    const size_t smem = sizeof(double) * (1024 + s->ch_win);
+    switch (s->ch_width) {
+        case 4: k_chain_solve<PRE, 4><<<ntasks, 32, smem, st>>>(A); break;
+        case 8: k_chain_solve<PRE, 8><<<ntasks, 32, smem, st>>>(A); break;
+        case 16: k_chain_solve<PRE, 16><<<ntasks, 32, smem, st>>>(A); break;
+        default: k_chain_solve<PRE, 32><<<ntasks, 32, smem, st>>>(A); break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    s->launches++;
+    return SPK_OK;
+}
+
+template <typename T>
+int upload_vec(DBuf<T> &d, const std::vector<T> &h) {
+    SPK_TRY(d.alloc(h.size()));
+    if (!h.empty()) SPK_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return SPK_OK;
+}
+
+int spike_firsts(spk_system *s, const std::vector<int2> &chains, std::vector<int> &first) {
+    DBuf<int2> d_ch;
+    DBuf<int> d_first;
+    SPK_TRY(upload_vec(d_ch, chains));
+    SPK_TRY(d_first.alloc(chains.size()));
+    SpikeArgs A;
+    A.chains = d_ch.p;
+    A.nchains = (int)chains.size();
+    A.val = s->ch_val.p;
+    A.off = (const unsigned *)s->ch_off.p;
+    A.ptr = s->ch_ptr.p;
+    A.reach = s->ch_reach;
+    A.tau = s->trunc_tol;
+    A.first = d_first.p;
+    const int C = s->ch_reach <= 32 ? 1 : (s->ch_reach <= 64 ? 2 : 4);
+    const int smem = (int)sizeof(double) * (s->ch_reach + 1) * 32 * C;
+    switch (C) {
+        case 1:
+            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_chain_spike<1><<<A.nchains, 32, smem, s->stream>>>(A);
+            break;
+        case 2:
+            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_chain_spike<2><<<A.nchains, 32, smem, s->stream>>>(A);
+            break;
+        default:
+            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            k_chain_spike<4><<<A.nchains, 32, smem, s->stream>>>(A);
+            break;
+    }
+    SPK_CUDA(cudaGetLastError());
+    first.assign(chains.size(), 0);
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    SPK_CUDA(cudaMemcpy(first.data(), d_first.p, sizeof(int) * chains.size(), cudaMemcpyDeviceToHost));
+    return SPK_OK;
+}
+
+void chain_release(spk_system *s) {
+    s->chain_ok = 0;
+    s->ch_val.release();
+    s->ch_off.release();
+    s->ch_ptr.release();
+    s->d_ctasks1.release();
+    s->d_ctasks4.release();
+    s->h_ctasks1.clear();
+    s->h_ctasks4.clear();
+    s->nctasks1 = s->nctasks4 = 0;
+    s->ch_rows1 = s->ch_rows4 = 0;
+    s->ch_count = 0;
+    s->ch_len = 0;
+}
+
+}  // namespace
+
+// Build the chain layout, the chains' spikes and the two task lists; leaves
+// chain_ok = 0 (the partition-based solve) when truncation is off, the layout
+// does not apply (column distance > 128, more than 32 off-diagonals in a row),
+// or no chain length up to the limit keeps every chain's first rows final.
+int chain_prepare(spk_system *s) {
+    chain_release(s);
+    const char *dis = getenv("SPK_DISABLE_CHAIN");  // test hook: force the partition-based solve
+    if (s->trunc_tol < 0 || (dis && dis[0] == '1') || s->n < 64) return SPK_OK;
+    const int n = s->n, ntiles = (n + 31) / 32;
+    std::vector<int> hw(ntiles);
+    int reach = 0;
+    {
+        DBuf<int> width, d_reach;
+        SPK_TRY(width.alloc(ntiles));
+        SPK_TRY(d_reach.alloc(1));
+        SPK_CUDA(cudaMemsetAsync(d_reach.p, 0, sizeof(int), s->stream));
+        k_chain_scan<<<nblocks(32ll * ntiles), 256, 0, s->stream>>>(n, s->uia.p, s->uja.p, width.p, d_reach.p);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaStreamSynchronize(s->stream));
+        SPK_CUDA(cudaMemcpy(hw.data(), width.p, sizeof(int) * ntiles, cudaMemcpyDeviceToHost));
+        SPK_CUDA(cudaMemcpy(&reach, d_reach.p, sizeof(int), cudaMemcpyDeviceToHost));
+    }
+    int wmax = 0;
+    std::vector<int> ptr(ntiles + 1, 0);
+    long long tot = 0;
+    for (int j = 0; j < ntiles; j++) {
+        const int wq = (hw[j] + 3) & ~3;
+        wmax = std::max(wmax, wq);
+        ptr[j] = (int)std::min<long long>(tot, 2147483647ll);
+        tot += 32ll * wq;
+    }
+    if (reach < 1 || reach > 128 || wmax > 32 || tot >= 2147483647ll) return SPK_OK;
+    ptr[ntiles] = (int)tot;
+    s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : 32));
+    s->ch_reach = reach;
+    int win = 64;
+    while (win < reach + 32) win <<= 1;
+    s->ch_win = win;
+    SPK_TRY(upload_vec(s->ch_ptr, ptr));
+    SPK_TRY(s->ch_val.alloc(std::max<long long>(tot, 2)));
+    SPK_TRY(s->ch_off.alloc(std::max<long long>(tot, 4)));
+    k_chain_fill<<<nblocks(32ll * ntiles), 256, 0, s->stream>>>(n, ntiles, s->uia.p, s->uja.p, s->ua.p,
+                                                                 s->ch_ptr.p, s->ch_val.p, s->ch_off.p);
+    SPK_CUDA(cudaGetLastError());
+
+    // chain length: about eight chains per SM, at least 1024 rows; doubled until valid
+    long long len = 32ll * ((n / (148 * 8) + 31) / 32);
+    len = std::max<long long>(len, 1024);
+    if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
+    const long long max_len = std::max<long long>(len, 32ll * ((n / 64 + 31) / 32));
+    for (; len <= max_len; len *= 2) {
+        std::vector<int2> chains;
+        for (long long a = 0; a < n; a += len)
+            chains.push_back(make_int2((int)a, (int)std::min<long long>(a + len, n)));
+        std::vector<int> first;
+        SPK_TRY(spike_firsts(s, chains, first));
+        bool ok = true;
+        for (size_t c = 1; c < chains.size() && ok; c++)
+            ok = first[c] >= std::min(chains[c].x + reach, chains[c].y);
+        if (!ok) continue;
+        std::vector<ChainTask> t1, t4;
+        long long rows1 = 0, rows4 = 0;
+        for (size_t c = 0; c < chains.size(); c++) {
+            const int a = chains[c].x, q = chains[c].y, f = first[c];
+            t1.push_back(ChainTask{a, q, a, f});
+            rows1 += q - a;
+            if (f < q) {
+                t4.push_back(ChainTask{f, q, f, q});
+                rows4 += q - f;
+            }
+        }
+        // both lists stay in row order: the pipelined solve launches them chunk by chunk
+        s->h_ctasks1 = t1;
+        s->h_ctasks4 = t4;
+        SPK_TRY(upload_vec(s->d_ctasks1, t1));
+        SPK_TRY(upload_vec(s->d_ctasks4, t4));
+        s->nctasks1 = (int)t1.size();
+        s->nctasks4 = (int)t4.size();
+        s->ch_rows1 = rows1;
+        s->ch_rows4 = rows4;
+        s->ch_count = (int)chains.size();
+        s->ch_len = (int)len;
+        s->chain_ok = 1;
+        return SPK_OK;
+    }
+    chain_release(s);
+    return SPK_OK;
+}
+
+// One solve of host arrays b and x through the chain path with the copies
+// overlapped: the rows are cut into chunks of whole chains (U order); chunk k's
+// right-hand side is copied in on s->st_in while earlier chunks are solved, its
+// phase 1 runs once it has landed, phase 4 of chunk k-1 follows phase 1 of
+// chunk k (it reads the first rows of the chain below), and each chunk's x is
+// copied out on s->st_out as soon as its phase 4 is done.  One cudaMemcpyAsync
+// per chunk and direction; overlap needs page-locked b and x (pageable memory
+// still gives the right result, with the copies serialised by the driver).
+int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx) {
+    const int n = s->n, nch = s->nctasks1;
+    int K = 8;
+    if (const char *e = getenv("SPK_PIPELINE_CHUNKS")) K = std::max(1, atoi(e));
+    K = std::min(K, std::max(nch, 1));
+    if (!s->st_in) {
+        SPK_CUDA(cudaStreamCreateWithFlags(&s->st_in, cudaStreamNonBlocking));
+        SPK_CUDA(cudaStreamCreateWithFlags(&s->st_out, cudaStreamNonBlocking));
+    }
+    for (int k = (int)s->pipe_ev.size(); k < 2 * K + 1; k++) {
+        cudaEvent_t e;
+        SPK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        s->pipe_ev.push_back(e);
+    }
+    cudaEvent_t *ev_in = s->pipe_ev.data(), *ev_done = ev_in + K, *ev_start = ev_in + 2 * K;
+    const bool rev = s->uplo == 'L';
+    // chunk k: chains [c0(k), c0(k+1)), U rows [A(k), Q(k)), phase-4 tasks [t0(k), t0(k+1))
+    std::vector<int> c0(K + 1), t0(K + 1, 0);
+    for (int k = 0; k <= K; k++) c0[k] = (int)((long long)nch * k / K);
+    {
+        int t = 0;
+        for (int k = 0; k < K; k++) {
+            t0[k] = t;
+            const int qend = s->h_ctasks1[c0[k + 1] - 1].hi;
+            while (t < s->nctasks4 && s->h_ctasks4[t].hi <= qend) t++;
+        }
+        t0[K] = s->nctasks4;
+    }
+    auto rows = [&](int k, int &A, int &Q) {
+        A = s->h_ctasks1[c0[k]].lo;
+        Q = s->h_ctasks1[c0[k + 1] - 1].hi;
+    };
+    // the copy streams start after everything queued on the system's stream
+    SPK_CUDA(cudaEventRecord(ev_start[0], s->stream));
+    SPK_CUDA(cudaStreamWaitEvent(s->st_in, ev_start[0], 0));
+    SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_start[0], 0));
+    for (int k = 0; k < K; k++) {
+        int A, Q;
+        rows(k, A, Q);
+        const int lo = rev ? n - Q : A;
+        SPK_CUDA(cudaMemcpyAsync(db + lo, b + lo, sizeof(double) * (Q - A), cudaMemcpyHostToDevice, s->st_in));
+        SPK_CUDA(cudaEventRecord(ev_in[k], s->st_in));
+    }
+    for (int k = 0; k <= K; k++) {
+        if (k < K) {
+            SPK_CUDA(cudaStreamWaitEvent(s->stream, ev_in[k], 0));
+            SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p + c0[k], c0[k + 1] - c0[k], db, dx, s->stream));
+        }
+        if (k >= 1) {
+            const int j = k - 1;
+            SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p + t0[j], t0[j + 1] - t0[j], db, dx, s->stream));
+            SPK_CUDA(cudaEventRecord(ev_done[j], s->stream));
+            int A, Q;
+            rows(j, A, Q);
+            const int lo = rev ? n - Q : A;
+            SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_done[j], 0));
+            SPK_CUDA(cudaMemcpyAsync(x + lo, dx + lo, sizeof(double) * (Q - A), cudaMemcpyDeviceToHost, s->st_out));
+        }
+    }
+    SPK_CUDA(cudaStreamSynchronize(s->st_out));
+    SPK_CUDA(cudaStreamSynchronize(s->st_in));
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return SPK_OK;
+}
+
+// One solve through the chain path: phase 1 then phase 4 on stream st.
+int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring) {
+    SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p, s->nctasks1, b, x, st));
+    if (prof) {
+        cudaEventRecord(s->ev[ring][1], st);
+        cudaEventRecord(s->ev[ring][2], st);
+    }
+    SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p, s->nctasks4, b, x, st));
+    return SPK_OK;
+}
+
+}  // namespace spk

@@ -83,6 +83,16 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
     return ok != 0;
 }
 
+// After a timed-out barrier wait: give the bulk copy still addressed to this
+// CTA's shared memory (parity `parity` of barrier `bar`) a second bounded period
+// to land, so that the CTA does not exit while a copy writes into its shared
+// memory.  Returns either way (a copy that never lands cannot be cancelled).
+__device__ __noinline__ void drain_copy(unsigned long long *bar, unsigned parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1ll << 32)) return;
+}
+
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -134,6 +144,7 @@ struct SegArgs {
     int rev_in;           // rhs[i] holds row n-1-i of U
     int rev_out;          // xout is stored in the caller's order with reversal
     int *err;
+    int fail_entry;       // test hook: take the timed-out-wait exit before any copy
 };
 
 // Lane 0: stage tile [r0, top) whose nonzeros are [e0, e1): the reciprocals of
@@ -242,6 +253,8 @@ __device__ bool solve_range(const SegArgs &A, SegSmem &S, unsigned &phase, int l
             const long long t0 = clock64();
             while (!mbar_try_wait(&S.bar[slot], (phase >> slot) & 1u)) {
                 if (clock64() - t0 > kWaitCycles) {
+                    drain_copy(&S.bar[slot], (phase >> slot) & 1u);
+                    if (it + 1 < ntiles) drain_copy(&S.bar[slot ^ 1], (phase >> (slot ^ 1)) & 1u);
                     if (lane == 0) atomicExch(A.err, 1);
                     return false;
                 }
@@ -339,6 +352,10 @@ __global__ void __launch_bounds__(32) k_segment_solve(SegArgs A) {
     const int task = blockIdx.x;
     if (task >= A.ntasks) return;
     const int lane = threadIdx.x;
+    if (A.fail_entry) {
+        if (lane == 0) atomicExch(A.err, 1);
+        return;
+    }
     if (lane == 0) {
         mbar_init(&S.bar[0], 1);
         mbar_init(&S.bar[1], 1);
@@ -412,6 +429,7 @@ struct TileArgs {
     int rev_out;
     int acc;              // right-hand-side-parallel phase 3+4: xout += x (needs couplings within the window)
     int *err;
+    int fail_entry;       // test hook: take the timed-out-wait exit before any copy
 };
 
 // Lane 0: stage tile j (entries [e0, e1)): its diagonal reciprocals and its first
@@ -472,6 +490,8 @@ __device__ bool tile_range(const TileArgs &A, TileSmemK<K, T> &S, unsigned &phas
             const long long t0 = clock64();
             while (!mbar_try_wait(&S.bar[slot], (phase >> slot) & 1u)) {
                 if (clock64() - t0 > kWaitCycles) {
+                    drain_copy(&S.bar[slot], (phase >> slot) & 1u);
+                    if (it + 1 < ntiles) drain_copy(&S.bar[slot ^ 1], (phase >> (slot ^ 1)) & 1u);
                     if (lane == 0) atomicExch(A.err, 1);
                     return false;
                 }
@@ -678,6 +698,10 @@ __device__ __forceinline__ void tile_task(const TileArgs &A, int task) {
     __shared__ TileSmemK<K, T> S;
     if (task >= A.ntasks) return;
     const int lane = threadIdx.x;
+    if (A.fail_entry) {
+        if (lane == 0) atomicExch(A.err, 1);
+        return;
+    }
     if (lane == 0) {
         mbar_init(&S.bar[0], 1);
         mbar_init(&S.bar[1], 1);
@@ -929,6 +953,7 @@ __device__ bool rhs_range(const TileArgs &A, RhsSmem<T> &S, unsigned &phase, int
             const long long t0 = clock64();
             while (!mbar_try_wait(&S.bar, phase)) {
                 if (clock64() - t0 > kWaitCycles) {
+                    drain_copy(&S.bar, phase);
                     if (lane == 0) atomicExch(A.err, 1);
                     return false;
                 }
@@ -1078,6 +1103,10 @@ __global__ void __launch_bounds__(32) k_rhs_solve(TileArgs A, int nk) {
     const int task = blockIdx.x;
     if (task >= A.ntasks) return;
     const int lane = threadIdx.x;
+    if (A.fail_entry) {
+        if (lane == 0) atomicExch(A.err, 1);
+        return;
+    }
     if (lane == 0) {
         mbar_init(&S.bar, 1);
         fence_mbar_init();
@@ -1857,7 +1886,7 @@ int solve_prepare(spk_system *s) {
     SPK_CUDA(cudaStreamSynchronize(s->stream));
     SPK_TRY(s->d_err.alloc(1));
     SPK_CUDA(cudaMemset(s->d_err.p, 0, sizeof(int)));
-    return SPK_OK;
+    return chain_prepare(s);
 }
 
 namespace {
@@ -1878,6 +1907,7 @@ int launch_tiles(spk_system *s, const double *rhs, long long ldb, double *xo, lo
     A.ldb = ldb;
     A.rev_in = s->uplo == 'L';
     A.err = s->d_err.p;
+    A.fail_entry = s->dbg_fail_waits > 0;
     if (s->redNec && s->ntasks1) {
         A.tasks = s->d_tasks1.p;
         A.ntasks = s->ntasks1;
@@ -1938,6 +1968,7 @@ int launch_rhs(spk_system *s, int nk, const double *rhs, long long ldb, double *
     A.ldb = ldb;
     A.rev_in = s->uplo == 'L';
     A.err = s->d_err.p;
+    A.fail_entry = s->dbg_fail_waits > 0;
     if (s->redNec && s->ntasks1) {
         A.tasks = s->d_tasks1.p;
         A.ntasks = s->ntasks1;
@@ -2100,7 +2131,9 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         if (s->ev_pending[ring]) SPK_TRY(collect_event_set(s, ring));
         cudaEventRecord(s->ev[ring][0], st);
     }
-    if (s->ell_ok && !ph) {
+    if (s->chain_ok && !ph) {
+        SPK_TRY(chain_solve(s, b, x, st, prof, ring));
+    } else if (s->ell_ok && !ph) {
         SPK_TRY((launch_tiles<1, double>(s, b, s->n, x, s->n, s->xbuf.p, st, prof, ring)));
     } else {
         // CSR segment solver (or the timed legacy path, which times the phases)
@@ -2113,6 +2146,7 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         A.rhs = b;
         A.rev_in = s->uplo == 'L';
         A.err = s->d_err.p;
+        A.fail_entry = s->dbg_fail_waits > 0;
         TileArgs TA{};
         TA.ell_val = s->ell_val.p;
         TA.ell_col = s->ell_col.p;
@@ -2123,6 +2157,7 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         TA.ldb = s->n;
         TA.rev_in = s->uplo == 'L';
         TA.err = s->d_err.p;
+        TA.fail_entry = s->dbg_fail_waits > 0;
         if (s->redNec && s->ntasks1) {
             A.tasks = TA.tasks = s->d_tasks1.p;
             A.ntasks = TA.ntasks = s->ntasks1;
@@ -2295,6 +2330,8 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     }
     if (iters) *iters = max_it;
     if (resid) *resid = worst;
+    // a call that waited for its residuals reports a failed device wait too
+    if (resid || (mode != 0 && tol >= 0)) SPK_TRY(check_device_error(s));
     return SPK_OK;
 }
 
@@ -2403,6 +2440,7 @@ int check_device_error(spk_system *s) {
     SPK_CUDA(cudaMemcpy(&e, s->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
         SPK_CUDA(cudaMemset(s->d_err.p, 0, sizeof(int)));
+        s->dbg_fail_waits = 0;  // the test hook (spk_debug_set "fail_waits") ends once reported
         set_error(SPK_ERR_TIMEOUT, "a bounded wait in the segment solver gave up");
         return SPK_ERR_TIMEOUT;
     }

@@ -99,6 +99,13 @@ struct SegTask {
     int tail;
 };
 
+// One warp's job in the chain solver: rows [lo, hi) of U bottom-up (hi is a
+// multiple of 32 or n), storing rows [st_lo, st_hi) into x.
+struct ChainTask {
+    int lo, hi;
+    int st_lo, st_hi;
+};
+
 // Truncation threshold on absolute spike-row sums (2^-60, below FP64 resolution
 // relative to ||x||_inf); negative = exact mode (nothing dropped).
 constexpr double kDefaultTruncTol = 8.673617379884035e-19;
@@ -145,8 +152,20 @@ struct spk_system {
     spk::DBuf<double> stage_b, stage_x;  // device copies of host b / x for spk_solve
     char *ext_ws = nullptr;  // caller-lent device workspace for the batched solves (spk_set_workspace)
     size_t ext_ws_bytes = 0;  // largest column distance from a tile's first row (-1: not computed)
+    // chain solver (default one-right-hand-side solve; chain.cu)
+    int chain_ok = 0, ch_width = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0;
+    spk::DBuf<double> ch_val;          // row-scaled off-diagonals, sliced ELL
+    spk::DBuf<unsigned char> ch_off;   // column offsets c - r (8 bits)
+    spk::DBuf<int> ch_ptr;             // first slot of each 32-row tile
+    spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;
+    int nctasks1 = 0, nctasks4 = 0;
+    long long ch_rows1 = 0, ch_rows4 = 0;
+    std::vector<spk::ChainTask> h_ctasks1, h_ctasks4;
+    cudaStream_t st_in = nullptr, st_out = nullptr;  // copy streams of the pipelined host-array solve
+    std::vector<cudaEvent_t> pipe_ev;
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
+    int dbg_fail_waits = 0;  // test hook: solve kernels report a failed wait at entry (spk_debug_set)
     // optional per-phase device timing (spk_set_profiling)
     int profiling = 0;
     static constexpr int kEvRing = 64;           // event sets in flight before a forced collection
@@ -170,6 +189,9 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
 int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
                        cudaStream_t st);
 int solve_prepare(spk_system *s);
+int chain_prepare(spk_system *s);
+int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
+int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);
 int check_device_error(spk_system *s);
 int collect_phase_times(spk_system *s);
 int collect_event_set(spk_system *s, int k);

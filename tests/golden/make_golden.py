@@ -13,7 +13,12 @@ reference's globals that the structure tests compare).
 'L' cases run the reference's 'U' path on the reversal mirror J L J (the
 reference's own 'L' path is unimplemented, src/spike_pstrsv.c:234-237).
 
-Usage: python tests/golden/make_golden.py   (needs the reference tree)
+* ``--full``       adds the full-size banded cases (m = 4,194,304; 'L' and 'U' at
+  16, 64, 256 and 1024 partitions) to ``digest.json`` and stores the
+  reference's x at sampled rows in ``full_x_samples.npz`` (a few minutes and
+  ~25 GB of host memory: the reference keeps its pools in static arrays).
+
+Usage: python tests/golden/make_golden.py [--full]   (needs the reference tree)
 """
 from __future__ import annotations
 
@@ -102,5 +107,52 @@ def main():
         json.dump(dig, f, indent=1, sort_keys=True)
 
 
+def full_cases():
+    """The banded workload at full size (m = 4,194,304): 'L' and 'U' (the
+    transpose) at every swept partition count."""
+    L = synth.banded_lower(4194304, seed=0)
+    out = [(f"banded4194304_L_P{P}", L, P, "L", 1) for P in (16, 64, 256, 1024)]
+    U = synth.transpose(L)
+    out += [(f"banded4194304_U_P{P}", U, P, "U", 1) for P in (16, 64, 256, 1024)]
+    return out
+
+
+def x_sample_index(m: int) -> np.ndarray:
+    """Rows whose x values are stored for the full-size cases: every 997th row plus
+    the first and last 64 (where the mirror and the partition edges meet)."""
+    idx = np.concatenate([np.arange(0, m, 997), np.arange(64), np.arange(m - 64, m)])
+    return np.unique(idx)
+
+
+def main_full():
+    """Digests of every structure array for the full-size banded cases, merged into
+    digest.json, and the reference's x at sampled rows (full_x_samples.npz)."""
+    if not oracle.Reference.available():
+        raise SystemExit("oracle/_ref/libspike_ref.so is missing: make -C oracle ref")
+    path = os.path.join(HERE, "digest.json")
+    with open(path) as f:
+        dig = json.load(f)
+    spath = os.path.join(HERE, "full_x_samples.npz")
+    samples = dict(np.load(spath)) if os.path.exists(spath) else {}
+    for name, A, P, uplo, flb in full_cases():
+        x_true, b = synth.make_rhs(A, seed=0)
+        st, x = run_reference(A, P, uplo, flb, b)
+        rec = {"m": int(A.m), "nnz": int(A.nnz), "P": P, "uplo": uplo, "flb": flb,
+               "gen": name.split("_")[0], "x_ref_norm": float(np.linalg.norm(x)),
+               "x_ref_err_vs_true": float(np.linalg.norm(x - x_true) / np.linalg.norm(x_true)),
+               "arrays": {k: digest(v) for k, v in st.items() if isinstance(v, np.ndarray)},
+               "sizes": {k: int(v.size) for k, v in st.items() if isinstance(v, np.ndarray)},
+               "scalars": {k: int(v) for k, v in st.items() if not isinstance(v, np.ndarray)}}
+        dig[name] = rec
+        samples[name] = x[x_sample_index(A.m)]
+        print(name, rec["scalars"], "err vs x_true", rec["x_ref_err_vs_true"], flush=True)
+        with open(path, "w") as f:
+            json.dump(dig, f, indent=1, sort_keys=True)
+        np.savez_compressed(spath, **samples)
+
+
 if __name__ == "__main__":
-    main()
+    if "--full" in sys.argv:
+        main_full()
+    else:
+        main()

@@ -1,0 +1,133 @@
+"""The chain solver (the default one-right-hand-side solve when spike truncation
+is on) against the sequential FP64 substitution, x_true and the partition-based
+solve it replaces.
+
+Rows are cut into chains independent of the partition count; every chain's
+spike is computed at preprocessing and decides which rows phase 4 re-solves
+(chain.cu).  The reference state (partitions, pools, spikes, reduced system) is
+untouched, so the structure tests in test_gpu_parity.py hold as before."""
+import numpy as np
+import pytest
+
+import oracle
+import spike_pstrsv_b200 as spk
+from cases import random_cases, rel_err
+from spike_pstrsv_b200 import synth
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def gpu_system(A, P, uplo, flb=1):
+    return spk.System().preproc(A.a, A.ia, A.ja, A.m, P, uplo, flb)
+
+
+@pytest.mark.parametrize("uplo", ["L", "U"])
+@pytest.mark.parametrize("P", [1, 4, 64, 300])
+def test_chain_engages_and_matches_substitution(uplo, P):
+    L = synth.banded_lower(262144, seed=5)
+    A = L if uplo == "L" else synth.transpose(L)
+    x_true, b = synth.make_rhs(A, seed=5)
+    S = gpu_system(A, P, uplo)
+    assert S.scalar("chain") == 1
+    assert S.scalar("chains") >= 64                     # parallelism no longer set by P
+    assert S.scalar("chain_rows_phase4") < A.m // 2     # only the coupled rows are re-solved
+    x = S.solve(b)
+    xs = oracle.sequential_solve(A, b, uplo)
+    assert rel_err(x, xs) <= TOL
+    assert rel_err(x, x_true) <= TOL
+
+
+def test_chain_agrees_with_partition_solve(monkeypatch):
+    L = synth.banded_lower(200000, seed=7)
+    x_true, b = synth.make_rhs(L, seed=7)
+    S = gpu_system(L, 64, "L")
+    assert S.scalar("chain") == 1
+    monkeypatch.setenv("SPK_DISABLE_CHAIN", "1")
+    Q = gpu_system(L, 64, "L")
+    assert Q.scalar("chain") == 0
+    x, xq = S.solve(b), Q.solve(b)
+    assert rel_err(x, xq) <= 1e-15
+    E = gpu_system(L, 64, "L").set_truncation(-1.0)      # exact mode: reference phases, no chains
+    assert E.scalar("chain") == 0
+    assert rel_err(x, E.solve(b)) <= 1e-15
+
+
+@pytest.mark.parametrize("m", [100003, 4097, 1000])
+def test_chain_ragged_sizes(m):
+    """Row counts that are not multiples of the 32-row tile, and small systems
+    (which may keep the partition-based solve)."""
+    L = synth.banded_lower(m, seed=m)
+    x_true, b = synth.make_rhs(L, seed=1)
+    for uplo, A in (("L", L), ("U", synth.transpose(L))):
+        bb = b if uplo == "L" else synth.spmv(A, x_true)
+        S = gpu_system(A, 8, uplo)
+        x = S.solve(bb)
+        assert rel_err(x, oracle.sequential_solve(A, bb, uplo)) <= TOL, (uplo, S.scalar("chain"))
+
+
+@pytest.mark.parametrize("rows", [1024, 2048, 8192])
+def test_chain_lengths(monkeypatch, rows):
+    """Chains of several lengths (the length is doubled at preprocessing until
+    every chain keeps its first rows final)."""
+    monkeypatch.setenv("SPK_CHAIN_ROWS", str(rows))
+    L = synth.banded_lower(150000, seed=11)
+    x_true, b = synth.make_rhs(L, seed=11)
+    S = gpu_system(L, 16, "L")
+    assert S.scalar("chain") == 1 and S.scalar("chain_rows") >= rows
+    assert rel_err(S.solve(b), oracle.sequential_solve(L, b, "L")) <= TOL
+
+
+def test_chain_poisson_and_random():
+    """Inputs whose spikes decay slowly or not at all, and irregular random
+    matrices: whichever path preprocessing picks, x matches the substitution."""
+    L = synth.poisson2d_lower(128)
+    x_true, b = synth.make_rhs(L, seed=0)
+    for P in (1, 4, 16):
+        S = gpu_system(L, P, "L")
+        assert rel_err(S.solve(b), oracle.sequential_solve(L, b, "L")) <= TOL
+    for name, A, P in random_cases(12, base_seed=77):
+        S = gpu_system(A, P, "U")
+        _, bb = synth.make_rhs(A, seed=3)
+        assert rel_err(S.solve(bb), oracle.sequential_solve(A, bb, "U")) <= TOL, name
+
+
+def test_chain_repeat_and_legacy_api():
+    """Repeated solves are identical (no state kept between calls) and the
+    reference-facing entry point (host arrays: copies overlapped with the chain
+    kernels) gives the same x."""
+    L = synth.banded_lower(131072, seed=2)
+    x_true, b = synth.make_rhs(L, seed=2)
+    S = gpu_system(L, 32, "L")
+    x1 = S.solve(b)
+    x2 = S.solve(b)
+    assert np.array_equal(x1, x2)
+    spk.spike_pstrsv_preproc(L.a, L.ia, L.ja, L.m, 32, "L")
+    for _ in range(2):
+        x = np.zeros(L.m)
+        spk.spike_pstrsv_solve("L", L.m, b.copy(), x, 32)
+        assert rel_err(x, x1) <= 1e-15
+
+
+@pytest.mark.parametrize("chunks", ["1", "3", "64"])
+def test_pipelined_host_solve(monkeypatch, chunks):
+    """The host-array solve in 1, 3 and 64 copy chunks (page-locked and pageable
+    buffers) against the device-resident solve, 'L' and 'U'."""
+    import torch
+
+    monkeypatch.setenv("SPK_PIPELINE_CHUNKS", chunks)
+    L = synth.banded_lower(300000, seed=8)
+    for uplo, A in (("L", L), ("U", synth.transpose(L))):
+        x_true, b = synth.make_rhs(A, seed=8)
+        S = gpu_system(A, 16, uplo)
+        assert S.scalar("chain") == 1
+        db = torch.from_numpy(b).cuda()
+        dx = torch.zeros_like(db)
+        S.solve(db, dx)
+        xd = dx.cpu().numpy()
+        bh = torch.from_numpy(b).pin_memory()
+        xh = torch.zeros(A.m, dtype=torch.float64).pin_memory()
+        S.solve(bh.numpy(), xh.numpy())
+        assert np.array_equal(xh.numpy(), xd)
+        assert np.array_equal(S.solve(b), xd)
+        assert rel_err(xd, x_true) <= TOL
