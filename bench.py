@@ -15,10 +15,15 @@ A step is one solve (spike_pstrsv_solve) of that system.
   e2e    : solves/s through the reference-facing C ABI (spike_pstrsv_solve)
            with pinned host buffers: every step copies b host->device and x
            device->host inside the timed region.
-  roofline: algorithmic bytes of the rows the segment-solver launches solve
-           (12 nnz + 4 (rows+1) + 16 rows per solve, i.e. B/m per row with
-           B = 12 nnz + 4 (m+1) + 16 m) over their event-timed duration,
-           against the measured HBM copy bandwidth.
+  roofline: the algorithmic bytes of one solve, B = 12 nnz + 4 (m+1) + 16 m
+           (each matrix byte once; the second pass over the coupled rows is not
+           credited), over the solve kernels' event-timed duration per solve,
+           against the measured HBM copy bandwidth.  kernel_rows_gbs credits
+           B/m per row each launch solves (rows solved twice count twice).
+  sweep  : the same workload at 16/64/256/1024 partitions, uplo L and U, with
+           spike truncation (default) and in exact mode (the reference's
+           phases: D1 sweep, reduced system, D2 sweep).
+  latency: the small Poisson 128x128 system at 4 partitions.
   cpu_baseline: the reference's own OpenMP code (oracle/_ref, built from the
            reference sources) on a bounded sample of the same workload.
 
@@ -114,6 +119,127 @@ def run_batched(S, L, x_true_k, dev, stream, k: int, mode: int, steps: int, warm
             "ms_per_batch": ms, "solves_per_s": k * 1e3 / ms, "hbm_gbs": nb / (ms * 1e-3) / 1e9,
             "algorithmic_bytes_per_batch": nb, "scaled_residual": resid, "rel_err_vs_x_true": err,
             "gpu_launches_per_batch": launches / steps}
+
+
+def node0_cpus():
+    """CPUs of NUMA node 0 (sysfs), for pinning the reference's OpenMP threads the
+    way its experiment script pins them to one node."""
+    try:
+        txt = open("/sys/devices/system/node/node0/cpulist").read().strip()
+    except OSError:
+        return None
+    cpus = set()
+    for part in txt.split(","):
+        if "-" in part:
+            a, b = part.split("-")
+            cpus.update(range(int(a), int(b) + 1))
+        elif part:
+            cpus.add(int(part))
+    return sorted(cpus)
+
+
+def kernel_time_per_solve(S, db, dx, sp, dev, n):
+    """Per-phase device time of n solves (events on the solve stream), ms per solve."""
+    import torch
+    S.set_profiling(True)
+    for _ in range(n):
+        S.solve_device(db.data_ptr(), dx.data_ptr(), sp)
+    torch.cuda.synchronize(dev)
+    ph, nsol = S.phase_times()
+    S.set_profiling(False)
+    return [p / max(nsol, 1) for p in ph]
+
+
+def timed_solves(S, db, dx, sp, stream, dev, warmup, steps):
+    import torch
+    for _ in range(warmup):
+        S.solve_device(db.data_ptr(), dx.data_ptr(), sp)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        S.solve_device(db.data_ptr(), dx.data_ptr(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    S.check()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_sweep(L, dev, stream, peak, steps: int = 30):
+    """Every partition count and uplo of the banded workload, default (spike
+    truncation) and exact mode, device-resident, CUDA-event timed."""
+    import torch
+    import spike_pstrsv_b200 as spk
+    from spike_pstrsv_b200 import synth
+    B = alg_bytes(L.m, L.nnz)
+    sp = stream.cuda_stream
+    out = []
+    for uplo in ("L", "U"):
+        A = L if uplo == "L" else synth.transpose(L)
+        x_true, b = synth.make_rhs(A, seed=0)
+        db = torch.from_numpy(b).to(dev)
+        dx = torch.zeros_like(db)
+        for P in (16, 64, 256, 1024):
+            t0 = time.perf_counter()
+            S = spk.System().preproc(A.a, A.ia, A.ja, A.m, P, uplo, 1)
+            pre_s = time.perf_counter() - t0
+            for exact in (False, True):
+                if exact:
+                    S.set_truncation(-1.0)
+                n = steps if not exact else max(3, steps // 6)
+                ms = timed_solves(S, db, dx, sp, stream, dev, 3, n)
+                x = dx.cpu().numpy()
+                cell = {"uplo": uplo, "partitions": P, "mode": "exact" if exact else "default",
+                        "solves_per_s": 1e3 / ms, "ms_per_solve": ms,
+                        "frac": B / (ms * 1e-3) / 1e9 / peak,
+                        "scaled_residual": scaled_residual(A, x, b),
+                        "rel_err_vs_x_true": float(np.linalg.norm(x - x_true) / np.linalg.norm(x_true)),
+                        "solver": "chain" if S.scalar("chain") else "partition",
+                        "launches_per_solve": S.scalar("launches_per_solve")}
+                if exact:
+                    cell["reduced_rows_kept"] = S.scalar("kept_reduced_rows")
+                    ph = kernel_time_per_solve(S, db, dx, sp, dev, n)
+                    cell["phases_ms"] = {"d1_local": ph[0], "reduced": ph[1], "d2_coupled": ph[2]}
+                else:
+                    cell["preprocess_s"] = pre_s
+                    cell["chains"] = S.scalar("chains")
+                out.append(cell)
+            S.close()
+            del S
+            torch.cuda.empty_cache()
+    return out
+
+
+def run_latency(dev, stream, steps: int = 200):
+    """The small Poisson 128x128 lower-triangular system (m = 16,384) at 4
+    partitions: device time per solve back to back, and the wall time of one
+    synchronous call with host arrays."""
+    import torch
+    import spike_pstrsv_b200 as spk
+    from spike_pstrsv_b200 import synth
+    L = synth.poisson2d_lower(128)
+    x_true, b = synth.make_rhs(L, seed=0)
+    S = spk.System().preproc(L.a, L.ia, L.ja, L.m, 4, "L", 1)
+    db = torch.from_numpy(b).to(dev)
+    dx = torch.zeros_like(db)
+    ms = timed_solves(S, db, dx, stream.cuda_stream, stream, dev, 10, steps)
+    x = np.zeros(L.m)
+    walls = []
+    for k in range(steps // 2 + 10):
+        t0 = time.perf_counter()
+        S.solve(b, x)
+        if k >= 10:
+            walls.append(time.perf_counter() - t0)
+    walls.sort()
+    out = {"workload": "Poisson 128x128 lower triangle, m=16384, nnz=48896, uplo=L, 4 partitions",
+           "device_us_per_solve": ms * 1e3,
+           "host_call_us_p50": 1e6 * walls[len(walls) // 2],
+           "host_call_us_p99": 1e6 * walls[int(0.99 * (len(walls) - 1))],
+           "rel_err_vs_x_true": float(np.linalg.norm(x - x_true) / np.linalg.norm(x_true)),
+           "solver": "chain" if S.scalar("chain") else "partition"}
+    S.close()
+    return out
 
 
 def peaks():
@@ -232,10 +358,23 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libspike_ref.so (the reference sources built here) is missing"}))
         return 0
+    cpus = node0_cpus()
+    pin = "none"
+    if cpus and hasattr(os, "sched_setaffinity"):
+        # one NUMA node, as the reference's experiment script pins with numactl
+        # (numactl itself is not installed; memory placement is left to first touch)
+        os.sched_setaffinity(0, cpus)
+        pin = f"node0 cpus {cpus[0]}-{cpus[-1]} ({len(cpus)}) via sched_setaffinity"
     L = synth.banded_lower(M_FULL, seed=0)
     _, b = synth.make_rhs(L, seed=0)
     U = synth.mirror(L)
     bu = b[::-1].copy()
+    # the single-core sequential substitution (the profiler's udsol/ldsol baseline)
+    seq = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        oracle.sequential_solve(L, b, "L")
+        seq.append(time.perf_counter() - t0)
     R = oracle.Reference()
     t0 = time.perf_counter()
     R.preproc(U, args.P, flb=1)
@@ -269,6 +408,9 @@ def run_reference(args):
                             "sample": f"full workload, {len(times)} timed solves after {args.warmup} warm-up, "
                                       f"b re-copied outside the timer; preprocessing {pre_s:.1f} s untimed"},
            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "pinning": pin,
+           "sequential_1core": {"solves_per_s": 1.0 / min(seq), "ms_per_solve": 1e3 * min(seq),
+                                "what": "forward substitution, one thread (the profiler's ldsol comparator), best of 3"},
            "accuracy": {"scaled_residual": res}}
     print(json.dumps(out))
     return 0
@@ -327,27 +469,26 @@ def run_ours(args):
     ms_max = max_over_ranks(ms, dev, world)
     value = replicas_value(ms_max, world)
 
-    # dominant kernel: the segment-solver launches (phases 1 and 3+4), event-timed per phase
-    S.set_profiling(True)
-    for _ in range(args.steps):
-        S.solve_device(db.data_ptr(), dx.data_ptr(), sp)
-    torch.cuda.synchronize(dev)
-    ph, nsol = S.phase_times()
-    S.set_profiling(False)
-    ph = [p / max(nsol, 1) for p in ph]
-    rows1, rows4 = S.scalar("rows_phase1"), S.scalar("rows_phase4")
-    per_row = B / m
-    seg_ms = ph[0] + ph[2]
-    seg_bytes = per_row * (rows1 + rows4)
+    # the solve's kernels, event-timed per phase on the solve stream
+    ph = kernel_time_per_solve(S, db, dx, sp, dev, args.steps)
+    chain = S.scalar("chain") == 1
+    if chain:
+        rows1, rows4 = S.scalar("chain_rows_phase1"), S.scalar("chain_rows_phase4")
+        kernel = "k_chain_solve (phase 1 chain-local sweep + phase 4 re-solve of the coupled rows), 2 launches per solve"
+    else:
+        rows1, rows4 = S.scalar("rows_phase1"), S.scalar("rows_phase4")
+        kernel = "k_tile_solve (phase 1 D1 sweep + phase 3/4 coupled D2 sweep), 2 launches per solve"
+    kernel_ms = ph[0] + ph[1] + ph[2]
     peak, peak_kind = peaks()
-    achieved = seg_bytes / (seg_ms * 1e-3) / 1e9
+    achieved = B / (kernel_ms * 1e-3) / 1e9
+    kernel_rows_gbs = (B / m) * (rows1 + rows4) / (kernel_ms * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "tile_solve_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "chain_solve_traffic.json" if chain else "tile_solve_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             tr = json.load(f)
-        # DRAM bytes per launch of the segment-solver kernel, scaled from the ncu
-        # capture of the same kernel by rows solved (traffic grows with the rows)
+        # DRAM bytes per launch, scaled from the ncu capture of the same kernel by
+        # the rows each launch solves (traffic grows with the rows)
         traffic = (tr["phase1_dram_bytes_per_row"] * rows1 + tr["phase4_dram_bytes_per_row"] * rows4) / 2 / 1e9
 
     # end to end through the reference-facing C ABI with pinned host buffers
@@ -383,6 +524,10 @@ def run_ours(args):
     if world == 1 and not args.no_served:
         from spike_pstrsv_b200 import group
         systems = group.run(count=128, reps=5)
+    sweep = latency = None
+    if world == 1 and not args.no_sweep:
+        sweep = run_sweep(L, dev, stream, peak)
+        latency = run_latency(dev, stream)
     clk = clocks.stop()
 
     x = dx.cpu().numpy()
@@ -405,18 +550,26 @@ def run_ours(args):
                           "per_gpu": "each rank solves its own copy (weak scaling)"},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                            "kernel": "k_tile_solve (phase 1 D1 sweep + phase 3/4 coupled D2 sweep), 2 launches per solve",
+                            "kernel": kernel,
+                            "achieved_is": "algorithmic bytes of one solve (12 nnz + 4 (m+1) + 16 m, each matrix "
+                                           "byte once) / event-timed kernel time per solve",
                             "traffic_unit": "GB per launch (ncu DRAM bytes per row x rows, averaged over the 2 launches)",
                             "algorithmic_bytes_per_solve": B,
-                            "whole_solve_gbs": B / (ms_max * 1e-3) / 1e9},
-               "phases_ms": {"d1_local": ph[0], "reduced": ph[1], "d2_coupled": ph[2],
-                             "rows_phase1": rows1, "rows_phase4": rows4},
+                            "kernel_ms_per_solve": kernel_ms,
+                            "kernel_rows_gbs": kernel_rows_gbs,
+                            "whole_solve_gbs": B / (ms_max * 1e-3) / 1e9,
+                            "whole_solve_frac": B / (ms_max * 1e-3) / 1e9 / peak},
+               "phases_ms": {"phase1": ph[0], "reduced": ph[1], "phase4": ph[2],
+                             "rows_phase1": rows1, "rows_phase4": rows4, "solver": "chain" if chain else "partition",
+                             "chains": S.scalar("chains")},
                "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * m,
                        "d2h_bytes_per_step": 8 * m, "api": "spike_pstrsv_solve (C ABI), pinned host b/x"},
                "gpu_launches": int(launches),
                "batched": batched,
                "served": served,
                "batched_systems": systems,
+               "sweep": sweep,
+               "latency_small": latency,
                "clocks": clk,
                "accuracy": {"scaled_residual": res, "rel_err_vs_x_true": err_true,
                             "e2e_vs_device_rel_diff": err_e2e}}
@@ -437,6 +590,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--P", type=int, default=1024, help="nthreads = Spike partitions")
     ap.add_argument("--no-served", action="store_true", help="skip the serving-loop stream")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the partition/uplo/exact sweep and latency")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
