@@ -2402,9 +2402,15 @@ int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, 
     }
     double *work = nullptr;
     SPK_TRY(static_scratch(&work));
+    // the same choice as solve_batch: the right-hand-side-parallel solver only
+    // when the tasks fill the GPU (two per SM), else tile groups of up to 16
+    int dev = 0, sms = 148;
+    SPK_CUDA(cudaGetDevice(&dev));
+    SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const bool wide_ok = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms;
     for (int g = 0; g < nrhs;) {
         const int left = nrhs - g;
-        int K = 32;
+        int K = wide_ok ? 32 : 16;
         while (K > 1 && (K > left || K * n > kStaticScratch)) K >>= 1;
         const double *Bg = B + g * ldb;
         double *Xg = X + g * ldx;
