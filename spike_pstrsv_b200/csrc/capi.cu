@@ -105,6 +105,7 @@ void destroy_system(spk_system *s) {
             if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     for (cudaEvent_t e : s->pipe_ev) cudaEventDestroy(e);
+    for (cudaStream_t q : s->pipe_st) cudaStreamDestroy(q);
     if (s->st_in) cudaStreamDestroy(s->st_in);
     if (s->st_out) cudaStreamDestroy(s->st_out);
     delete s;

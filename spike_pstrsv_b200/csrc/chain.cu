@@ -25,13 +25,14 @@
 // Kernel.  One warp per task, lane = row of a 32-row tile, tiles bottom-up.  The
 // matrix is stored for this solver as a sliced ELL of ROW-SCALED off-diagonals
 // a(r,c)/a(r,r) (so x_r = b_r/a(r,r) - sum v'(r,c) x_c) with 8-bit column
-// offsets c - r, per tile slot-pair-major (values: one 16-byte load per lane
-// per two slots; offsets: one 4-byte load per lane per four slots).  Each tile
-// is loaded straight into registers two tiles ahead, so shared memory carries
-// only the solved-row window (gathers of far columns) and a per-lane column of
+// offsets c - r, per tile slot-pair-major (values: one 16-byte copy per lane per
+// two slots; offsets: one 4-byte copy per lane per four slots).  Each tile is
+// staged into shared memory by cp.async two tiles ahead; every lane copies and
+// reads only its own row, so a stage needs no barrier.  Shared memory also holds
+// the solved-row window (gathers of far columns) and a per-lane column of
 // in-tile coefficients: coef[i][lane] = v'(row0+lane, row0+i) is written and
-// read by its own lane only, so the in-tile triangle needs no barrier beyond
-// the warp shuffles that broadcast each solved row.
+// read by its own lane only, so the in-tile triangle needs no barrier beyond the
+// warp shuffles that broadcast each solved row.
 //
 // Memory per solve (banded workload, 16 off-diagonals per row): 16 x 9 B of
 // matrix + 8 B 1/diagonal + 8 B b + 8 B x per row in phase 1, the same per
@@ -40,6 +41,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 #include "spk_internal.cuh"
@@ -196,51 +198,92 @@ struct ChainArgs {
     double *x;          // caller order
     int rev;            // uplo 'L': caller row i is U row n-1-i
     int mask;           // window rows - 1 (power of two >= reach + 32)
+    int sw;             // slots of the widest tile (stage size)
     int *err;
     int fail_entry;     // test hook: report a failed wait and return (spk_debug_set "fail_waits")
 };
 
-template <int W>
-struct TileRegs {
-    double2 v[W / 2];
-    unsigned o[W / 4];
-    double b, rd;
-    int w;  // slots of this tile (multiple of 4)
+// cp.async (sm_80+): per-thread asynchronous global -> shared copies, tracked
+// by commit groups (no register scoreboard, so a tile in flight never stalls
+// the tile being solved)
+__device__ __forceinline__ void cpa16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr int kChainStages = 3;  // tiles in shared memory: the one solved + two in flight
+
+// One staged tile (sw = the widest tile's slots, a multiple of 4).  Lane l
+// copies (and later reads) only its own row: value pairs v[(k/2)*32 + l],
+// offset words o[(k/4)*32 + l], rd[l], b[l].
+struct ChainStage {
+    double2 *v;   // [16 sw]
+    double *rd;   // [32]
+    double *b;    // [32]
+    unsigned *o;  // [8 sw]
 };
 
+__host__ __device__ __forceinline__ int chain_stage_bytes(int sw) { return 288 * sw + 512; }
+
+__device__ __forceinline__ ChainStage chain_stage(unsigned char *base, int s, int sw) {
+    unsigned char *p = base + (size_t)s * chain_stage_bytes(sw);
+    ChainStage S;
+    S.v = (double2 *)p;
+    S.rd = (double *)(p + 256 * sw);
+    S.b = S.rd + 32;
+    S.o = (unsigned *)(p + 256 * sw + 512);
+    return S;
+}
+
 template <int W>
-__device__ __forceinline__ void load_tile(const ChainArgs &A, TileRegs<W> &R, int j, int p0, int p1, int lo, int hi,
-                                          int lane) {
-    R.w = (p1 - p0) >> 5;
+__device__ __forceinline__ void stage_tile(const ChainArgs &A, const ChainStage &S, int j, int wq, int p0, int lo,
+                                           int hi, int lane) {
     const double2 *vp = (const double2 *)(A.val + p0) + lane;
     const unsigned *op = A.off + (p0 >> 2) + lane;
 #pragma unroll
     for (int k = 0; k < W / 2; k++)
-        if (2 * k < R.w) R.v[k] = __ldg(vp + 32 * k);
+        if (2 * k < wq) cpa16(&S.v[32 * k + lane], vp + 32 * k);
 #pragma unroll
     for (int k = 0; k < W / 4; k++)
-        if (4 * k < R.w) R.o[k] = __ldg(op + 32 * k);
+        if (4 * k < wq) cpa4(&S.o[32 * k + lane], op + 32 * k);
     const int r = 32 * j + lane;
-    const bool act = r >= lo && r < hi;
-    R.b = act ? __ldg(A.b + (A.rev ? A.n - 1 - r : r)) : 0.0;
-    R.rd = act ? __ldg(A.rd + r) : 0.0;
+    if (r >= lo && r < hi) {
+        cpa8(&S.rd[lane], A.rd + r);
+        cpa8(&S.b[lane], A.b + (A.rev ? A.n - 1 - r : r));
+    }
 }
 
 template <int W>
-__device__ __forceinline__ void solve_tile(const ChainArgs &A, const TileRegs<W> &R, int j, const ChainTask &t,
-                                           double *coef, double *win, int lane) {
+__device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage &S, int wq, int j,
+                                           const ChainTask &t, double *coef, double *win, int lane) {
     const int row0 = 32 * j, r = row0 + lane;
     const bool act = r >= t.lo && r < t.hi;
-    double acc = R.b * R.rd;
+    double acc = act ? S.b[lane] * S.rd[lane] : 0.0;
     double p[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned ow[W / 4];
+#pragma unroll
+    for (int k = 0; k < W / 4; k++) ow[k] = 4 * k < wq ? S.o[32 * k + lane] : 0u;
     // far columns from the window, in-tile columns into the lane's coefficient column
 #pragma unroll
-    for (int k = 0; k < W; k++) {
-        if (4 * (k >> 2) < R.w) {
-            const int o = (R.o[k >> 2] >> (8 * (k & 3))) & 0xff;
-            const double v = (k & 1) ? R.v[k >> 1].y : R.v[k >> 1].x;
-            const int d = lane + o;
-            if (act) {
+    for (int k2 = 0; k2 < W / 2; k2++) {
+        if (2 * k2 < wq && act) {
+            const double2 v2 = S.v[32 * k2 + lane];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int k = 2 * k2 + h;
+                const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
+                const double v = h ? v2.y : v2.x;
                 if (d < 32) coef[d * 32 + lane] = v;
                 else p[k & 3] = fma(v, win[(row0 + d) & A.mask], p[k & 3]);
             }
@@ -259,8 +302,8 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const TileRegs<W>
         // leave the coefficient column zero for the next tile
 #pragma unroll
         for (int k = 0; k < W; k++) {
-            if (4 * (k >> 2) < R.w) {
-                const int d = lane + ((R.o[k >> 2] >> (8 * (k & 3))) & 0xff);
+            if (k < wq) {
+                const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
                 if (d < 32) coef[d * 32 + lane] = 0.0;
             }
         }
@@ -272,10 +315,12 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const TileRegs<W>
 // phase 1 (it starts at zero: zero coupling beyond the chain).
 template <bool PRE, int W>
 __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
-    constexpr int NS = W <= 16 ? 3 : 2;  // register stages: tiles in flight = NS - 1
-    extern __shared__ double sm[];
-    double *coef = sm;        // [32 columns][32 lanes]
-    double *win = sm + 1024;  // [mask + 1]
+    extern __shared__ __align__(16) unsigned char smc[];
+    ChainStage stg[kChainStages];
+#pragma unroll
+    for (int s = 0; s < kChainStages; s++) stg[s] = chain_stage(smc, s, A.sw);
+    double *coef = (double *)(smc + kChainStages * chain_stage_bytes(A.sw));  // [32 columns][32 lanes]
+    double *win = coef + 1024;                                                // [mask + 1]
     const int lane = threadIdx.x;
     if (A.fail_entry) {
         if (lane == 0) atomicExch(A.err, 1);
@@ -292,39 +337,52 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     }
     __syncwarp();
     const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
-    // tile jj uses register stage (jt - jj) % NS; its pointers are loaded one
-    // iteration before its slots, its slots NS - 1 iterations before it is solved
-    TileRegs<W> R[NS];
-    int P0[NS], P1[NS];
+    // slot counts of the tiles, 32 at a time: lane l holds tile (base - l)'s
+    auto ptr_pair = [&](int base, int &p0, int &p1) {
+        const int jj = base - lane;
+        p0 = jj >= jb ? __ldg(A.ptr + jj) : 0;
+        p1 = jj >= jb ? __ldg(A.ptr + jj + 1) : 0;
+    };
+    int pbase = jt, pa, pb;
+    ptr_pair(pbase, pa, pb);
+    auto tile_ptr = [&](int jj, int &p0, int &wq) {
+        if (pbase - jj >= 32) {  // uniform: the next 32 tiles' pointers
+            pbase -= 32;
+            ptr_pair(pbase, pa, pb);
+        }
+        p0 = __shfl_sync(kFull, pa, pbase - jj);
+        wq = (__shfl_sync(kFull, pb, pbase - jj) - p0) >> 5;
+    };
+    int wq_st[kChainStages];
 #pragma unroll
-    for (int s = 0; s < NS; s++) {
+    for (int s = 0; s < kChainStages - 1; s++) {
         const int jj = jt - s;
         if (jj >= jb) {
-            P0[s] = __ldg(A.ptr + jj);
-            P1[s] = __ldg(A.ptr + jj + 1);
+            int p0;
+            tile_ptr(jj, p0, wq_st[s]);
+            stage_tile<W>(A, stg[s], jj, wq_st[s], p0, t.lo, t.hi, lane);
         }
+        cpa_commit();
     }
+    for (int j0 = jt; j0 >= jb; j0 -= kChainStages) {
 #pragma unroll
-    for (int s = 0; s < NS - 1; s++)
-        if (jt - s >= jb) load_tile<W>(A, R[s], jt - s, P0[s], P1[s], t.lo, t.hi, lane);
-    for (int j0 = jt; j0 >= jb; j0 -= NS) {
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
+        for (int s = 0; s < kChainStages; s++) {
             const int j = j0 - s;
             if (j >= jb) {
-                const int sl = (s + NS - 1) % NS;  // stage of tile j - (NS - 1)
-                const int jl = j - (NS - 1);
-                if (jl >= jb) load_tile<W>(A, R[sl], jl, P0[sl], P1[sl], t.lo, t.hi, lane);
-                // pointers of tile j - NS into this tile's stage (its own are consumed)
-                const int jp = j - NS;
-                if (jp >= jb) {
-                    P0[s] = __ldg(A.ptr + jp);
-                    P1[s] = __ldg(A.ptr + jp + 1);
+                const int sl = (s + kChainStages - 1) % kChainStages;  // stage of tile j - 2
+                const int jl = j - (kChainStages - 1);
+                if (jl >= jb) {
+                    int p0;
+                    tile_ptr(jl, p0, wq_st[sl]);
+                    stage_tile<W>(A, stg[sl], jl, wq_st[sl], p0, t.lo, t.hi, lane);
                 }
-                solve_tile<W>(A, R[s], j, t, coef, win, lane);
+                cpa_commit();
+                cpa_wait<kChainStages - 1>();  // this tile's copies have landed (own lane's)
+                solve_tile<W>(A, stg[s], wq_st[s], j, t, coef, win, lane);
             }
         }
     }
+    cpa_wait<0>();
 }
 
 template <bool PRE>
@@ -341,16 +399,220 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.x = x;
     A.rev = s->uplo == 'L';
     A.mask = s->ch_win - 1;
+    A.sw = s->ch_sw;
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
-    const size_t smem = sizeof(double) * (1024 + s->ch_win);
+    auto go = [&](auto kern) -> int {
+        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (1024 + s->ch_win);
+        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<ntasks, 32, smem, st>>>(A);
+        SPK_CUDA(cudaGetLastError());
+        return SPK_OK;
+    };
     switch (s->ch_width) {
-        case 4: k_chain_solve<PRE, 4><<<ntasks, 32, smem, st>>>(A); break;
-        case 8: k_chain_solve<PRE, 8><<<ntasks, 32, smem, st>>>(A); break;
-        case 16: k_chain_solve<PRE, 16><<<ntasks, 32, smem, st>>>(A); break;
-        default: k_chain_solve<PRE, 32><<<ntasks, 32, smem, st>>>(A); break;
+        case 4: SPK_TRY(go(k_chain_solve<PRE, 4>)); break;
+        case 8: SPK_TRY(go(k_chain_solve<PRE, 8>)); break;
+        case 16: SPK_TRY(go(k_chain_solve<PRE, 16>)); break;
+        case 32: SPK_TRY(go(k_chain_solve<PRE, 32>)); break;
+        default: SPK_TRY(go(k_chain_solve<PRE, 64>)); break;
     }
-    SPK_CUDA(cudaGetLastError());
+    s->launches++;
+    return SPK_OK;
+}
+
+// ---- many right-hand sides: lane = right-hand side ---------------------------------------
+//
+// The same chains and tasks, up to 32 right-hand sides per warp: lane k owns
+// right-hand side k and walks the task's rows bottom-up, so every window access
+// of a lane is to its own column and the row-to-row dependency needs no
+// barrier.  The window [row mod W][33] (T) holds x of solved rows and, for the
+// tile in flight, its right-hand sides: a tile's b rows are loaded coalesced
+// along rows (lane = row) one tile ahead and transposed into the window, and a
+// solved tile's x rows leave the same way.  The tile's slots (values in T,
+// offsets) are staged row-major in shared memory, so that a row's slots are
+// broadcast loads; they are loaded one tile ahead into registers.
+// Per row and right-hand side: one window value per slot (8 or 4 bytes of
+// shared memory), one fused multiply-add.
+
+constexpr int kRhsPad = 33;
+
+template <typename T>
+struct RhsArgs {
+    const ChainTask *tasks;
+    const T *val;          // row-scaled values in T, chain layout
+    const unsigned *off;
+    const int *ptr;
+    const T *rd;           // 1 / diagonal in T
+    int n;
+    const double *B;       // caller order, column-major
+    long long ldb;
+    double *X;             // caller order, column-major (FP64 output)
+    long long ldx;
+    int rev;
+    int nk;                // right-hand sides in this pass (<= 32)
+    int mask;
+    int *err;
+    int fail_entry;
+};
+
+template <typename T, int W>
+struct RhsTile {
+    typename std::conditional<sizeof(T) == 8, double2, float2>::type v[W / 2];
+    unsigned o[W / 4];
+    T rd;
+    int w;
+};
+
+template <typename T, int W>
+__device__ __forceinline__ void rhs_load_tile(const RhsArgs<T> &A, RhsTile<T, W> &R, int j, int lane) {
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    const int p0 = __ldg(A.ptr + j), p1 = __ldg(A.ptr + j + 1);
+    R.w = (p1 - p0) >> 5;
+    const V2 *vp = (const V2 *)(A.val + p0) + lane;
+    const unsigned *op = A.off + (p0 >> 2) + lane;
+#pragma unroll
+    for (int k = 0; k < W / 2; k++)
+        if (2 * k < R.w) R.v[k] = vp[32 * k];
+#pragma unroll
+    for (int k = 0; k < W / 4; k++)
+        if (4 * k < R.w) R.o[k] = __ldg(op + 32 * k);
+    R.rd = A.rd[min(32 * j + lane, A.n - 1)];
+}
+
+// right-hand sides of tile row 32j + lane, all columns (rows outside [lo, hi): 0)
+template <typename T>
+__device__ __forceinline__ void rhs_load_b(const RhsArgs<T> &A, double (&bv)[32], int j, int lo, int hi, int lane) {
+    const int r = 32 * j + lane;
+    const bool ok = r >= lo && r < hi;
+    const long long o = A.rev ? (long long)A.n - 1 - r : r;
+#pragma unroll
+    for (int k = 0; k < 32; k++) bv[k] = (ok && k < A.nk) ? A.B[k * A.ldb + o] : 0.0;
+}
+
+template <typename T, int W, bool PRE>
+__global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    constexpr int SW = W + 2;               // staged row stride (elements): conflict-free stores
+    T *win = (T *)smraw;                    // [mask + 1][kRhsPad]
+    T *sv = win + (A.mask + 1) * kRhsPad;   // [32][SW] values, row-major
+    unsigned *so = (unsigned *)(sv + 32 * SW);  // [32][W/4 + 1] offsets
+    T *srd = (T *)(so + 32 * (W / 4 + 1));  // [32] 1/diagonal
+    constexpr int SO = W / 4 + 1;
+    const int lane = threadIdx.x;
+    if (A.fail_entry) {
+        if (lane == 0) atomicExch(A.err, 1);
+        return;
+    }
+    const ChainTask t = A.tasks[blockIdx.x];
+    const int n = A.n;
+    // window: the rows above the task (phase 4: x from phase 1; phase 1: zero)
+    for (int i = lane; i <= A.mask; i += 32) {
+        const int r = t.hi + i;
+        const bool ok = PRE && r < n;
+        const long long o = A.rev ? (long long)n - 1 - r : r;
+        T *wr = win + (r & A.mask) * kRhsPad;
+#pragma unroll 4
+        for (int k = 0; k < 32; k++) wr[k] = (ok && k < A.nk) ? (T)A.X[k * A.ldx + o] : T(0);
+    }
+    const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
+    RhsTile<T, W> cur;
+    double bv[32];
+    rhs_load_tile<T, W>(A, cur, jt, lane);
+    rhs_load_b<T>(A, bv, jt, t.lo, t.hi, lane);
+    for (int j = jt; j >= jb; j--) {
+        const int row0 = 32 * j;
+        const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
+        __syncwarp();  // the previous tile's x rows have been read out of the window
+        // stage this tile: slots row-major, right-hand sides into the window rows
+#pragma unroll
+        for (int k = 0; k < W / 2; k++)
+            if (2 * k < cur.w) *reinterpret_cast<V2 *>(sv + lane * SW + 2 * k) = cur.v[k];
+#pragma unroll
+        for (int k = 0; k < W / 4; k++)
+            if (4 * k < cur.w) so[lane * SO + k] = cur.o[k];
+        srd[lane] = cur.rd;
+        {
+            T *wr = win + ((row0 + lane) & A.mask) * kRhsPad;
+#pragma unroll
+            for (int k = 0; k < 32; k++) wr[k] = (T)bv[k];
+        }
+        const int w = cur.w;
+        // next tile into registers while this one is solved
+        if (j - 1 >= jb) {
+            rhs_load_tile<T, W>(A, cur, j - 1, lane);
+            rhs_load_b<T>(A, bv, j - 1, t.lo, t.hi, lane);
+        }
+        __syncwarp();
+        for (int r = a1 - 1; r >= a0; r--) {
+            const int i = r - row0;
+            T acc = win[(r & A.mask) * kRhsPad + lane] * srd[i];
+            T p[2] = {T(0), T(0)};
+#pragma unroll
+            for (int k4 = 0; k4 < W / 4; k4++) {
+                if (4 * k4 < w) {
+                    const unsigned ow = so[i * SO + k4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int c = r + ((ow >> (8 * u)) & 0xff);
+                        const T v = sv[i * SW + 4 * k4 + u];
+                        p[u & 1] = fma(v, win[(c & A.mask) * kRhsPad + lane], p[u & 1]);
+                    }
+                }
+            }
+            acc -= p[0] + p[1];
+            win[(r & A.mask) * kRhsPad + lane] = acc;
+        }
+        __syncwarp();
+        // x rows of this tile out (lane = row), for the rows this task stores
+        {
+            const int r = row0 + lane;
+            if (r >= a0 && r < a1 && r >= t.st_lo && r < t.st_hi) {
+                const long long o = A.rev ? (long long)n - 1 - r : r;
+                const T *wr = win + (r & A.mask) * kRhsPad;
+#pragma unroll 8
+                for (int k = 0; k < 32; k++)
+                    if (k < A.nk) A.X[k * A.ldx + o] = (double)wr[k];
+            }
+        }
+    }
+}
+
+template <typename T, bool PRE>
+int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, const double *B, long long ldb,
+                     double *X, long long ldx, cudaStream_t st) {
+    if (ntasks <= 0) return SPK_OK;
+    RhsArgs<T> A;
+    A.tasks = tasks;
+    A.val = sizeof(T) == 8 ? (const T *)(const void *)s->ch_val.p : (const T *)(const void *)s->ch_valf.p;
+    A.off = (const unsigned *)s->ch_off.p;
+    A.ptr = s->ch_ptr.p;
+    A.rd = sizeof(T) == 8 ? (const T *)(const void *)s->rdiag.p : (const T *)(const void *)s->rdiagf.p;
+    A.n = s->n;
+    A.B = B;
+    A.ldb = ldb;
+    A.X = X;
+    A.ldx = ldx;
+    A.rev = s->uplo == 'L';
+    A.nk = nk;
+    A.mask = s->ch_win - 1;
+    A.err = s->d_err.p;
+    A.fail_entry = s->dbg_fail_waits > 0;
+    const int W = s->ch_width;
+    const size_t smem = sizeof(T) * ((size_t)s->ch_win * kRhsPad + 32 * (W + 2) + 32) + 4 * 32 * (W / 4 + 1) + 64;
+    auto go = [&](auto kern) -> int {
+        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<ntasks, 32, smem, st>>>(A);
+        SPK_CUDA(cudaGetLastError());
+        return SPK_OK;
+    };
+    switch (W) {
+        case 4: SPK_TRY(go(k_chain_rhs<T, 4, PRE>)); break;
+        case 8: SPK_TRY(go(k_chain_rhs<T, 8, PRE>)); break;
+        case 16: SPK_TRY(go(k_chain_rhs<T, 16, PRE>)); break;
+        case 32: SPK_TRY(go(k_chain_rhs<T, 32, PRE>)); break;
+        default: SPK_TRY(go(k_chain_rhs<T, 64, PRE>)); break;
+    }
     s->launches++;
     return SPK_OK;
 }
@@ -399,9 +661,29 @@ int spike_firsts(spk_system *s, const std::vector<int2> &chains, std::vector<int
     return SPK_OK;
 }
 
+__global__ void k_chain_to_float(long long n, const double *__restrict__ a, float *__restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// FP32 copies of the chain values and of 1/diagonal (made on first use)
+int chain_fp32(spk_system *s) {
+    if (s->ch_valf.p) return SPK_OK;
+    SPK_TRY(s->ch_valf.alloc(s->ch_val.n));
+    if (!s->rdiagf.p) {
+        SPK_TRY(s->rdiagf.alloc(s->rdiag.n));
+        k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->rdiag.n, s->rdiag.p, s->rdiagf.p);
+    }
+    k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->ch_val.n, s->ch_val.p, s->ch_valf.p);
+    SPK_CUDA(cudaGetLastError());
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return SPK_OK;
+}
+
 void chain_release(spk_system *s) {
     s->chain_ok = 0;
     s->ch_val.release();
+    s->ch_valf.release();
     s->ch_off.release();
     s->ch_ptr.release();
     s->d_ctasks1.release();
@@ -418,7 +700,7 @@ void chain_release(spk_system *s) {
 
 // Build the chain layout, the chains' spikes and the two task lists; leaves
 // chain_ok = 0 (the partition-based solve) when truncation is off, the layout
-// does not apply (column distance > 128, more than 32 off-diagonals in a row),
+// does not apply (column distance > 128, more than 64 off-diagonals in a row),
 // or no chain length up to the limit keeps every chain's first rows final.
 int chain_prepare(spk_system *s) {
     chain_release(s);
@@ -447,9 +729,10 @@ int chain_prepare(spk_system *s) {
         ptr[j] = (int)std::min<long long>(tot, 2147483647ll);
         tot += 32ll * wq;
     }
-    if (reach < 1 || reach > 128 || wmax > 32 || tot >= 2147483647ll) return SPK_OK;
+    if (reach < 1 || reach > 128 || wmax > 64 || tot >= 2147483647ll) return SPK_OK;
     ptr[ntiles] = (int)tot;
-    s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : 32));
+    s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : (wmax <= 32 ? 32 : 64)));
+    s->ch_sw = wmax;
     s->ch_reach = reach;
     int win = 64;
     while (win < reach + 32) win <<= 1;
@@ -506,28 +789,34 @@ int chain_prepare(spk_system *s) {
 }
 
 // One solve of host arrays b and x through the chain path with the copies
-// overlapped: the rows are cut into chunks of whole chains (U order); chunk k's
-// right-hand side is copied in on s->st_in while earlier chunks are solved, its
-// phase 1 runs once it has landed, phase 4 of chunk k-1 follows phase 1 of
-// chunk k (it reads the first rows of the chain below), and each chunk's x is
-// copied out on s->st_out as soon as its phase 4 is done.  One cudaMemcpyAsync
-// per chunk and direction; overlap needs page-locked b and x (pageable memory
-// still gives the right result, with the copies serialised by the driver).
+// overlapped: the rows are cut into chunks of whole chains (U order), each with
+// a stream of its own.  Chunk k's right-hand side is copied in on s->st_in; its
+// phase 1 starts on its stream once that copy has landed (chunks run side by
+// side: a chain is a serial walk, so one chunk alone leaves most SMs idle);
+// its phase 4 waits for phase 1 of chunk k+1 (it reads the first rows of the
+// chain below); its x is copied out on s->st_out once its phase 4 is done.  One
+// cudaMemcpyAsync per chunk and direction; overlap needs page-locked b and x
+// (pageable memory gives the same result with the copies serialised).
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx) {
     const int n = s->n, nch = s->nctasks1;
-    int K = 8;
+    int K = 16;
     if (const char *e = getenv("SPK_PIPELINE_CHUNKS")) K = std::max(1, atoi(e));
     K = std::min(K, std::max(nch, 1));
     if (!s->st_in) {
         SPK_CUDA(cudaStreamCreateWithFlags(&s->st_in, cudaStreamNonBlocking));
         SPK_CUDA(cudaStreamCreateWithFlags(&s->st_out, cudaStreamNonBlocking));
     }
-    for (int k = (int)s->pipe_ev.size(); k < 2 * K + 1; k++) {
+    while ((int)s->pipe_st.size() < K) {
+        cudaStream_t q;
+        SPK_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        s->pipe_st.push_back(q);
+    }
+    while ((int)s->pipe_ev.size() < 3 * K + 1) {
         cudaEvent_t e;
         SPK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         s->pipe_ev.push_back(e);
     }
-    cudaEvent_t *ev_in = s->pipe_ev.data(), *ev_done = ev_in + K, *ev_start = ev_in + 2 * K;
+    cudaEvent_t *ev_in = s->pipe_ev.data(), *ev_p1 = ev_in + K, *ev_done = ev_in + 2 * K, *ev_start = ev_in + 3 * K;
     const bool rev = s->uplo == 'L';
     // chunk k: chains [c0(k), c0(k+1)), U rows [A(k), Q(k)), phase-4 tasks [t0(k), t0(k+1))
     std::vector<int> c0(K + 1), t0(K + 1, 0);
@@ -541,40 +830,61 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
         }
         t0[K] = s->nctasks4;
     }
-    auto rows = [&](int k, int &A, int &Q) {
-        A = s->h_ctasks1[c0[k]].lo;
-        Q = s->h_ctasks1[c0[k + 1] - 1].hi;
+    auto lo_rows = [&](int k, int &lo, int &cnt) {
+        const int A = s->h_ctasks1[c0[k]].lo, Q = s->h_ctasks1[c0[k + 1] - 1].hi;
+        lo = rev ? n - Q : A;
+        cnt = Q - A;
     };
-    // the copy streams start after everything queued on the system's stream
+    // everything starts after the work already queued on the system's stream
     SPK_CUDA(cudaEventRecord(ev_start[0], s->stream));
     SPK_CUDA(cudaStreamWaitEvent(s->st_in, ev_start[0], 0));
     SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_start[0], 0));
     for (int k = 0; k < K; k++) {
-        int A, Q;
-        rows(k, A, Q);
-        const int lo = rev ? n - Q : A;
-        SPK_CUDA(cudaMemcpyAsync(db + lo, b + lo, sizeof(double) * (Q - A), cudaMemcpyHostToDevice, s->st_in));
+        int lo, cnt;
+        lo_rows(k, lo, cnt);
+        SPK_CUDA(cudaMemcpyAsync(db + lo, b + lo, sizeof(double) * cnt, cudaMemcpyHostToDevice, s->st_in));
         SPK_CUDA(cudaEventRecord(ev_in[k], s->st_in));
     }
-    for (int k = 0; k <= K; k++) {
-        if (k < K) {
-            SPK_CUDA(cudaStreamWaitEvent(s->stream, ev_in[k], 0));
-            SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p + c0[k], c0[k + 1] - c0[k], db, dx, s->stream));
-        }
-        if (k >= 1) {
-            const int j = k - 1;
-            SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p + t0[j], t0[j + 1] - t0[j], db, dx, s->stream));
-            SPK_CUDA(cudaEventRecord(ev_done[j], s->stream));
-            int A, Q;
-            rows(j, A, Q);
-            const int lo = rev ? n - Q : A;
-            SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_done[j], 0));
-            SPK_CUDA(cudaMemcpyAsync(x + lo, dx + lo, sizeof(double) * (Q - A), cudaMemcpyDeviceToHost, s->st_out));
-        }
+    for (int k = 0; k < K; k++) {
+        cudaStream_t q = s->pipe_st[k];
+        SPK_CUDA(cudaStreamWaitEvent(q, ev_in[k], 0));
+        SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p + c0[k], c0[k + 1] - c0[k], db, dx, q));
+        SPK_CUDA(cudaEventRecord(ev_p1[k], q));
     }
+    for (int k = 0; k < K; k++) {
+        cudaStream_t q = s->pipe_st[k];
+        if (k + 1 < K) SPK_CUDA(cudaStreamWaitEvent(q, ev_p1[k + 1], 0));
+        SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p + t0[k], t0[k + 1] - t0[k], db, dx, q));
+        SPK_CUDA(cudaEventRecord(ev_done[k], q));
+        int lo, cnt;
+        lo_rows(k, lo, cnt);
+        SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_done[k], 0));
+        SPK_CUDA(cudaMemcpyAsync(x + lo, dx + lo, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s->st_out));
+    }
+    // the system's stream continues after the whole solve
+    SPK_CUDA(cudaEventRecord(ev_start[0], s->st_out));
+    SPK_CUDA(cudaStreamWaitEvent(s->stream, ev_start[0], 0));
     SPK_CUDA(cudaStreamSynchronize(s->st_out));
-    SPK_CUDA(cudaStreamSynchronize(s->st_in));
-    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return SPK_OK;
+}
+
+// Up to 32 right-hand sides (device, column-major) through the chain path:
+// phase 1 then phase 4 of the right-hand-side-parallel chain kernel, in T
+// (double, or float with the FP32 copy of the values).  X is FP64.
+int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long ldb, double *X, long long ldx,
+                    cudaStream_t st) {
+    if (nk < 1 || nk > 32) {
+        set_error(SPK_ERR_ARG, "chain batch of %d columns (1..32)", nk);
+        return SPK_ERR_ARG;
+    }
+    if (fp32) {
+        SPK_TRY(chain_fp32(s));
+        SPK_TRY((launch_chain_rhs<float, false>(s, s->d_ctasks1.p, s->nctasks1, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<float, true>(s, s->d_ctasks4.p, s->nctasks4, nk, B, ldb, X, ldx, st)));
+    } else {
+        SPK_TRY((launch_chain_rhs<double, false>(s, s->d_ctasks1.p, s->nctasks1, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<double, true>(s, s->d_ctasks4.p, s->nctasks4, nk, B, ldb, X, ldx, st)));
+    }
     return SPK_OK;
 }
 

@@ -2239,7 +2239,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     const size_t col_bytes = ((size_t)32 * n * sizeof(double) + 255) / 256 * 256;
     char *work_p = nullptr;
     double *rbuf_p = nullptr, *dbuf_p = nullptr;
-    if (mode == 1) {
+    if (mode == 1 && !s->chain_ok) {
         SPK_TRY(ensure_fp32(s));
         SPK_TRY(ensure_reach(s));
     }
@@ -2273,6 +2273,48 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     SPK_CUDA(cudaGetDevice(&dev));
     SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const bool wide_ok = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms;
+    if (s->chain_ok) {
+        // the chain tasks fill the GPU whatever the partition count: every group
+        // of up to 32 columns is one right-hand-side-parallel chain solve
+        for (int g = 0; g < nrhs;) {
+            const int K = std::min(nrhs - g, 32);
+            const double *Bg = B + g * ldb;
+            double *Xg = X + g * ldx;
+            if (mode == 0) {
+                SPK_TRY(chain_solve_rhs(s, 0, K, Bg, ldb, Xg, ldx, st));
+                if (resid) {
+                    SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, rbuf_p, n, st, true));
+                    double r = 0;
+                    SPK_TRY(scaled_residual(s, K, st, &r));
+                    worst = worst_of(worst, r);
+                }
+            } else {
+                SPK_TRY(chain_solve_rhs(s, 1, K, Bg, ldb, Xg, ldx, st));
+                int it = 0;
+                double r = -1.0;
+                for (;; it++) {
+                    const bool check = tol >= 0 || (resid && it == maxit);
+                    if (tol < 0 && it == maxit && !resid) break;
+                    SPK_TRY(residual(s, K, Xg, ldx, Bg, ldb, rbuf_p, n, st, check));
+                    if (check) {
+                        SPK_TRY(scaled_residual(s, K, st, &r));
+                        if ((tol >= 0 && r <= tol) || it == maxit) break;
+                    }
+                    if (it == maxit) break;
+                    SPK_TRY(chain_solve_rhs(s, 1, K, rbuf_p, n, dbuf_p, n, st));
+                    k_axpy<<<dim3(148, K), 256, 0, st>>>(s->n, K, dbuf_p, Xg, ldx);
+                    SPK_CUDA(cudaGetLastError());
+                }
+                max_it = std::max(max_it, it);
+                if (!(r < 0)) worst = worst_of(worst, r);
+            }
+            g += K;
+        }
+        if (iters) *iters = max_it;
+        if (resid) *resid = worst;
+        if (resid || (mode != 0 && tol >= 0)) SPK_TRY(check_device_error(s));
+        return SPK_OK;
+    }
     for (int g = 0; g < nrhs;) {
         const int left = nrhs - g;
         // 17..32 columns: one right-hand-side-parallel pass (work holds 32 columns);

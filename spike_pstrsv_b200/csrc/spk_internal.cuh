@@ -153,8 +153,9 @@ struct spk_system {
     char *ext_ws = nullptr;  // caller-lent device workspace for the batched solves (spk_set_workspace)
     size_t ext_ws_bytes = 0;  // largest column distance from a tile's first row (-1: not computed)
     // chain solver (default one-right-hand-side solve; chain.cu)
-    int chain_ok = 0, ch_width = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0;
+    int chain_ok = 0, ch_width = 0, ch_sw = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0;
     spk::DBuf<double> ch_val;          // row-scaled off-diagonals, sliced ELL
+    spk::DBuf<float> ch_valf;          // their FP32 copy (batched FP32 solves, made on first use)
     spk::DBuf<unsigned char> ch_off;   // column offsets c - r (8 bits)
     spk::DBuf<int> ch_ptr;             // first slot of each 32-row tile
     spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;
@@ -163,6 +164,7 @@ struct spk_system {
     std::vector<spk::ChainTask> h_ctasks1, h_ctasks4;
     cudaStream_t st_in = nullptr, st_out = nullptr;  // copy streams of the pipelined host-array solve
     std::vector<cudaEvent_t> pipe_ev;
+    std::vector<cudaStream_t> pipe_st;  // one per chunk of the pipelined solve
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     int dbg_fail_waits = 0;  // test hook: solve kernels report a failed wait at entry (spk_debug_set)
@@ -192,6 +194,8 @@ int solve_prepare(spk_system *s);
 int chain_prepare(spk_system *s);
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);
+int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long ldb, double *X, long long ldx,
+                    cudaStream_t st);
 int check_device_error(spk_system *s);
 int collect_phase_times(spk_system *s);
 int collect_event_set(spk_system *s, int k);
