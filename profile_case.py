@@ -1,9 +1,11 @@
 """A small, self-contained solve workload for profiler captures (ncu) of the
-solve kernels.
+solve kernels.  Not part of the library: it drives the library the way a user
+would, so that a capture sees only the solve's own launches.
 
-    python -m spike_pstrsv_b200.profile_case --m 2097152 --P 512 --nrhs 1
-        plain FP64 solves (spk_solve_device; k_tile_solve with one right-hand side)
-    python -m spike_pstrsv_b200.profile_case --m 2097152 --P 512 --nrhs 32 --mode 1
+    python profile_case.py --m 2097152 --P 512 --nrhs 1
+        plain FP64 solves (spk_solve_device: k_chain_solve, or k_tile_solve with
+        --no-chain)
+    python profile_case.py --m 2097152 --P 512 --nrhs 32 --mode 1
         batched solves (spk_solve_batch; FP32 + one refinement step with mode 1)
 
 The system is the banded lower-triangular workload (16 of the 64 preceding
@@ -13,6 +15,10 @@ calls follow one warm-up call.
 from __future__ import annotations
 
 import argparse
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def main():
@@ -27,7 +33,10 @@ def main():
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--mode", type=int, default=0)
     ap.add_argument("--solves", type=int, default=3)
+    ap.add_argument("--no-chain", action="store_true", help="the partition-based solve (SPK_DISABLE_CHAIN=1)")
     args = ap.parse_args()
+    if args.no_chain:
+        os.environ["SPK_DISABLE_CHAIN"] = "1"
     L = synth.banded_lower(args.m)
     S = spk.System().preproc(L.a, L.ia, L.ja, L.m, args.P, "L", 1)
     st = torch.cuda.current_stream()

@@ -748,7 +748,8 @@ int chain_prepare(spk_system *s) {
     long long len = 32ll * ((n / (148 * 8) + 31) / 32);
     len = std::max<long long>(len, 1024);
     if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
-    const long long max_len = std::max<long long>(len, 32ll * ((n / 64 + 31) / 32));
+    // at most three doublings, and never fewer than 8 chains
+    const long long max_len = std::min<long long>(8 * len, std::max<long long>(len, 32ll * ((n / 8 + 31) / 32)));
     for (; len <= max_len; len *= 2) {
         std::vector<int2> chains;
         for (long long a = 0; a < n; a += len)
