@@ -274,38 +274,60 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
     unsigned ow[W / 4];
 #pragma unroll
     for (int k = 0; k < W / 4; k++) ow[k] = 4 * k < wq ? S.o[32 * k + lane] : 0u;
-    // far columns from the window, in-tile columns into the lane's coefficient column
+    // Every slot stores its value into the lane's coefficient column (in-tile
+    // columns at their row, the others into scratch row 32) and loads the
+    // window value at its column, kept only for far columns (a select, so that
+    // a stale slot of the window cannot leak in): no branch.
 #pragma unroll
     for (int k2 = 0; k2 < W / 2; k2++) {
-        if (2 * k2 < wq && act) {
+        if (2 * k2 < wq) {
             const double2 v2 = S.v[32 * k2 + lane];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int k = 2 * k2 + h;
                 const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
-                const double v = h ? v2.y : v2.x;
-                if (d < 32) coef[d * 32 + lane] = v;
-                else p[k & 3] = fma(v, win[(row0 + d) & A.mask], p[k & 3]);
+                const double v = act ? (h ? v2.y : v2.x) : 0.0;
+                const bool in = d < 32;
+                coef[(in ? d : 32) * 32 + lane] = v;
+                const double wv = win[(row0 + d) & A.mask];
+                const double f = fma(v, wv, p[k & 3]);
+                p[k & 3] = in ? p[k & 3] : f;
             }
         }
     }
     acc -= (p[0] + p[1]) + (p[2] + p[3]);
-    // in-tile triangle, bottom-up: row i is final when its lane broadcasts it
+    __syncwarp();  // the block coefficients below read other lanes' columns
+    // In-tile triangle, bottom-up, four rows per step: the four accumulators are
+    // broadcast together, every lane resolves the block's four unknowns from the
+    // block's six coefficients (uniform loads) and applies all four columns.  A
+    // lane's coefficients at or below its own row are zero, so lanes inside the
+    // block come out with their final values too.
 #pragma unroll
-    for (int i = 31; i >= 0; i--) {
-        const double xi = __shfl_sync(kFull, acc, i);
-        acc = fma(-coef[i * 32 + lane], xi, acc);
+    for (int i = 31; i >= 3; i -= 4) {
+        const double c0 = coef[i * 32 + lane], c1 = coef[(i - 1) * 32 + lane];
+        const double c2 = coef[(i - 2) * 32 + lane], c3 = coef[(i - 3) * 32 + lane];
+        const double u10 = coef[i * 32 + i - 1];
+        const double u20 = coef[i * 32 + i - 2], u21 = coef[(i - 1) * 32 + i - 2];
+        const double u30 = coef[i * 32 + i - 3], u31 = coef[(i - 1) * 32 + i - 3], u32 = coef[(i - 2) * 32 + i - 3];
+        const double b0 = __shfl_sync(kFull, acc, i), b1 = __shfl_sync(kFull, acc, i - 1);
+        const double b2 = __shfl_sync(kFull, acc, i - 2), b3 = __shfl_sync(kFull, acc, i - 3);
+        const double a1 = fma(-u10, b0, b1);
+        const double a2 = fma(-u21, a1, fma(-u20, b0, b2));
+        const double a3 = fma(-u32, a2, fma(-u31, a1, fma(-u30, b0, b3)));
+        const double t01 = fma(-c1, a1, fma(-c0, b0, acc));
+        acc = fma(-c3, a3, fma(-c2, a2, t01));
     }
+    __syncwarp();  // block coefficients read before the columns are cleared
     if (act) {
         win[r & A.mask] = acc;
         if (r >= t.st_lo && r < t.st_hi) A.x[A.rev ? A.n - 1 - r : r] = acc;
-        // leave the coefficient column zero for the next tile
+    }
+    // leave the coefficient column zero for the next tile (inactive lanes wrote zeros)
 #pragma unroll
-        for (int k = 0; k < W; k++) {
-            if (k < wq) {
-                const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
-                if (d < 32) coef[d * 32 + lane] = 0.0;
-            }
+    for (int k = 0; k < W; k++) {
+        if (k < wq) {
+            const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
+            if (d < 32) coef[d * 32 + lane] = 0.0;
         }
     }
     __syncwarp();
@@ -319,8 +341,8 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     ChainStage stg[kChainStages];
 #pragma unroll
     for (int s = 0; s < kChainStages; s++) stg[s] = chain_stage(smc, s, A.sw);
-    double *coef = (double *)(smc + kChainStages * chain_stage_bytes(A.sw));  // [32 columns][32 lanes]
-    double *win = coef + 1024;                                                // [mask + 1]
+    double *coef = (double *)(smc + kChainStages * chain_stage_bytes(A.sw));  // [33 rows][32 lanes]; row 32: scratch
+    double *win = coef + 33 * 32;                                             // [mask + 1]
     const int lane = threadIdx.x;
     if (A.fail_entry) {
         if (lane == 0) atomicExch(A.err, 1);
@@ -328,7 +350,7 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     }
     const ChainTask t = A.tasks[blockIdx.x];
 #pragma unroll
-    for (int i = 0; i < 32; i++) coef[i * 32 + lane] = 0.0;
+    for (int i = 0; i < 33; i++) coef[i * 32 + lane] = 0.0;
     for (int k = lane; k <= A.mask; k += 32) {
         const int r = t.hi + k;
         double v = 0.0;
@@ -403,7 +425,7 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     auto go = [&](auto kern) -> int {
-        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (1024 + s->ch_win);
+        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (33 * 32 + s->ch_win);
         SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntasks, 32, smem, st>>>(A);
         SPK_CUDA(cudaGetLastError());
