@@ -198,6 +198,7 @@ struct ChainArgs {
     double *x;          // caller order
     int rev;            // uplo 'L': caller row i is U row n-1-i
     int mask;           // window rows - 1 (power of two >= reach + 32)
+    int reach;          // widest column distance
     int sw;             // slots of the widest tile (stage size)
     int *err;
     int fail_entry;     // test hook: report a failed wait and return (spk_debug_set "fail_waits")
@@ -354,7 +355,7 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     for (int k = lane; k <= A.mask; k += 32) {
         const int r = t.hi + k;
         double v = 0.0;
-        if (PRE && r < A.n) v = A.x[A.rev ? A.n - 1 - r : r];  // rows >= hi + reach are loaded, never read
+        if (PRE && r < A.n && k < A.reach) v = A.x[A.rev ? A.n - 1 - r : r];  // the coupling rows only
         win[r & A.mask] = v;
     }
     __syncwarp();
@@ -421,6 +422,7 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.x = x;
     A.rev = s->uplo == 'L';
     A.mask = s->ch_win - 1;
+    A.reach = s->ch_reach;
     A.sw = s->ch_sw;
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
@@ -447,14 +449,14 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
 // The same chains and tasks, up to 32 right-hand sides per warp: lane k owns
 // right-hand side k and walks the task's rows bottom-up, so every window access
 // of a lane is to its own column and the row-to-row dependency needs no
-// barrier.  The window [row mod W][33] (T) holds x of solved rows and, for the
-// tile in flight, its right-hand sides: a tile's b rows are loaded coalesced
-// along rows (lane = row) one tile ahead and transposed into the window, and a
-// solved tile's x rows leave the same way.  The tile's slots (values in T,
-// offsets) are staged row-major in shared memory, so that a row's slots are
-// broadcast loads; they are loaded one tile ahead into registers.
-// Per row and right-hand side: one window value per slot (8 or 4 bytes of
-// shared memory), one fused multiply-add.
+// barrier.  The window [WR][33] (T, WR = reach + 32 rows, row r at r mod WR)
+// holds x of the solved rows.  A tile (32 rows) is staged by cp.async one tile
+// ahead, each lane copying its own row: the slot values (T) and offsets, 1/diag
+// and the row's right-hand sides b[row][0..nk) (FP64).  When a tile has landed,
+// each lane turns its row's offsets into window element indices (row of the
+// column mod WR, times 33), so that a slot in the row loop is one broadcast
+// index, one window load and one fused multiply-add.  Solved rows leave the
+// window through a transpose (lane = row, coalesced along rows).
 
 constexpr int kRhsPad = 33;
 
@@ -472,118 +474,149 @@ struct RhsArgs {
     long long ldx;
     int rev;
     int nk;                // right-hand sides in this pass (<= 32)
-    int mask;
+    int wr;                // window rows (>= reach + 32)
+    int reach;             // widest column distance
+    int sw;                // slots of the widest tile
     int *err;
     int fail_entry;
 };
 
-template <typename T, int W>
-struct RhsTile {
-    typename std::conditional<sizeof(T) == 8, double2, float2>::type v[W / 2];
-    unsigned o[W / 4];
-    T rd;
-    int w;
+template <typename T>
+struct RhsStage {
+    T *v;         // [32 sw] as copied: pair (k/2)*32 + l holds slots k, k+1 of row l
+    unsigned *o;  // [8 sw]  offset words (k/4)*32 + l
+    double *b;    // [32][33] right-hand sides, row-major
+    T *rd;        // [32]
 };
 
-template <typename T, int W>
-__device__ __forceinline__ void rhs_load_tile(const RhsArgs<T> &A, RhsTile<T, W> &R, int j, int lane) {
-    using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-    const int p0 = __ldg(A.ptr + j), p1 = __ldg(A.ptr + j + 1);
-    R.w = (p1 - p0) >> 5;
-    const V2 *vp = (const V2 *)(A.val + p0) + lane;
-    const unsigned *op = A.off + (p0 >> 2) + lane;
-#pragma unroll
-    for (int k = 0; k < W / 2; k++)
-        if (2 * k < R.w) R.v[k] = vp[32 * k];
-#pragma unroll
-    for (int k = 0; k < W / 4; k++)
-        if (4 * k < R.w) R.o[k] = __ldg(op + 32 * k);
-    R.rd = A.rd[min(32 * j + lane, A.n - 1)];
+__host__ __device__ __forceinline__ int rhs_stage_bytes(int sw, int tsize) {
+    return 32 * sw * tsize + 32 * sw + 32 * kRhsPad * 8 + 32 * 8;
 }
 
-// right-hand sides of tile row 32j + lane, all columns (rows outside [lo, hi): 0)
 template <typename T>
-__device__ __forceinline__ void rhs_load_b(const RhsArgs<T> &A, double (&bv)[32], int j, int lo, int hi, int lane) {
-    const int r = 32 * j + lane;
-    const bool ok = r >= lo && r < hi;
-    const long long o = A.rev ? (long long)A.n - 1 - r : r;
+__device__ __forceinline__ RhsStage<T> rhs_stage(unsigned char *base, int sw) {
+    RhsStage<T> S;
+    S.v = (T *)base;
+    S.o = (unsigned *)(base + 32 * sw * sizeof(T));
+    S.b = (double *)(base + 32 * sw * sizeof(T) + 32 * sw);
+    S.rd = (T *)(S.b + 32 * kRhsPad);
+    return S;
+}
+
+template <typename T, int W>
+__device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsStage<T> &S, int j, int p0, int wq,
+                                               int lo, int hi, int lane) {
+    const T *vp = A.val + p0 + 2 * lane;
+    const unsigned *op = A.off + (p0 >> 2) + lane;
 #pragma unroll
-    for (int k = 0; k < 32; k++) bv[k] = (ok && k < A.nk) ? A.B[k * A.ldb + o] : 0.0;
+    for (int k = 0; k < W / 2; k++) {
+        if (2 * k < wq) {
+            if (sizeof(T) == 8) cpa16(S.v + 64 * k + 2 * lane, vp + 64 * k);
+            else cpa8(S.v + 64 * k + 2 * lane, vp + 64 * k);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < W / 4; k++)
+        if (4 * k < wq) cpa4(S.o + 32 * k + lane, op + 32 * k);
+    const int r = 32 * j + lane;
+    if (r >= lo && r < hi) {
+        if (sizeof(T) == 8) cpa8(S.rd + lane, A.rd + r);
+        else cpa4(S.rd + lane, A.rd + r);
+        const long long o = A.rev ? (long long)A.n - 1 - r : r;
+        for (int k = 0; k < A.nk; k++) cpa8(S.b + lane * kRhsPad + k, A.B + k * A.ldb + o);
+    }
 }
 
 template <typename T, int W, bool PRE>
 __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
-    extern __shared__ __align__(16) unsigned char smraw[];
     using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-    constexpr int SW = W + 2;               // staged row stride (elements): conflict-free stores
-    T *win = (T *)smraw;                    // [mask + 1][kRhsPad]
-    T *sv = win + (A.mask + 1) * kRhsPad;   // [32][SW] values, row-major
-    unsigned *so = (unsigned *)(sv + 32 * SW);  // [32][W/4 + 1] offsets
-    T *srd = (T *)(so + 32 * (W / 4 + 1));  // [32] 1/diagonal
-    constexpr int SO = W / 4 + 1;
+    constexpr int WIP = W / 2 + 1;  // packed window indices per row (stride, words)
+    extern __shared__ __align__(16) unsigned char smr[];
     const int lane = threadIdx.x;
     if (A.fail_entry) {
         if (lane == 0) atomicExch(A.err, 1);
         return;
     }
+    const int WR = A.wr;
+    const int sb = rhs_stage_bytes(A.sw, sizeof(T));
+    unsigned *wi = (unsigned *)(smr + 2 * sb);                  // [32][WIP] two 16-bit indices per word
+    T *win = (T *)(smr + 2 * sb + ((32 * WIP * 4 + 15) & ~15));  // [WR][33]
     const ChainTask t = A.tasks[blockIdx.x];
     const int n = A.n;
-    // window: the rows above the task (phase 4: x from phase 1; phase 1: zero)
-    for (int i = lane; i <= A.mask; i += 32) {
+    // window: the coupling rows above the task (phase 4: x from phase 1; phase
+    // 1: zero); farther rows start at zero, so that no stale value is ever read
+    for (int i = lane; i < WR; i += 32) {
         const int r = t.hi + i;
-        const bool ok = PRE && r < n;
+        const bool ok = PRE && r < n && i < A.reach;
         const long long o = A.rev ? (long long)n - 1 - r : r;
-        T *wr = win + (r & A.mask) * kRhsPad;
-#pragma unroll 4
+        T *wr = win + (r % WR) * kRhsPad;
         for (int k = 0; k < 32; k++) wr[k] = (ok && k < A.nk) ? (T)A.X[k * A.ldx + o] : T(0);
     }
     const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
-    RhsTile<T, W> cur;
-    double bv[32];
-    rhs_load_tile<T, W>(A, cur, jt, lane);
-    rhs_load_b<T>(A, bv, jt, t.lo, t.hi, lane);
-    for (int j = jt; j >= jb; j--) {
-        const int row0 = 32 * j;
-        const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
-        __syncwarp();  // the previous tile's x rows have been read out of the window
-        // stage this tile: slots row-major, right-hand sides into the window rows
-#pragma unroll
-        for (int k = 0; k < W / 2; k++)
-            if (2 * k < cur.w) *reinterpret_cast<V2 *>(sv + lane * SW + 2 * k) = cur.v[k];
-#pragma unroll
-        for (int k = 0; k < W / 4; k++)
-            if (4 * k < cur.w) so[lane * SO + k] = cur.o[k];
-        srd[lane] = cur.rd;
-        {
-            T *wr = win + ((row0 + lane) & A.mask) * kRhsPad;
-#pragma unroll
-            for (int k = 0; k < 32; k++) wr[k] = (T)bv[k];
-        }
-        const int w = cur.w;
-        // next tile into registers while this one is solved
+    auto tile_ptr = [&](int jj, int &p0, int &wq) {
+        p0 = __ldg(A.ptr + jj);
+        wq = (__ldg(A.ptr + jj + 1) - p0) >> 5;
+    };
+    int p0n, wqn;
+    tile_ptr(jt, p0n, wqn);
+    rhs_stage_tile<T, W>(A, rhs_stage<T>(smr, A.sw), jt, p0n, wqn, t.lo, t.hi, lane);
+    cpa_commit();
+    int wq_cur = wqn;
+    if (jt - 1 >= jb) tile_ptr(jt - 1, p0n, wqn);
+    for (int j = jt, it = 0; j >= jb; j--, it++) {
+        const RhsStage<T> S = rhs_stage<T>(smr + (it & 1) * sb, A.sw);
+        const int wq = wq_cur;
         if (j - 1 >= jb) {
-            rhs_load_tile<T, W>(A, cur, j - 1, lane);
-            rhs_load_b<T>(A, bv, j - 1, t.lo, t.hi, lane);
+            rhs_stage_tile<T, W>(A, rhs_stage<T>(smr + ((it + 1) & 1) * sb, A.sw), j - 1, p0n, wqn, t.lo, t.hi, lane);
+            wq_cur = wqn;
+            if (j - 2 >= jb) tile_ptr(j - 2, p0n, wqn);
         }
-        __syncwarp();
-        for (int r = a1 - 1; r >= a0; r--) {
-            const int i = r - row0;
-            T acc = win[(r & A.mask) * kRhsPad + lane] * srd[i];
-            T p[2] = {T(0), T(0)};
+        cpa_commit();
+        cpa_wait<1>();
+        const int row0 = 32 * j;
+        const int base = row0 % WR;
+        // this lane's row: window element index of every slot's column
+        {
+            unsigned words[W / 2];
 #pragma unroll
             for (int k4 = 0; k4 < W / 4; k4++) {
-                if (4 * k4 < w) {
-                    const unsigned ow = so[i * SO + k4];
+                const unsigned ow = 4 * k4 < wq ? S.o[32 * k4 + lane] : 0u;
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        const int c = r + ((ow >> (8 * u)) & 0xff);
-                        const T v = sv[i * SW + 4 * k4 + u];
-                        p[u & 1] = fma(v, win[(c & A.mask) * kRhsPad + lane], p[u & 1]);
+                for (int h = 0; h < 2; h++) {
+                    unsigned pr = 0;
+#pragma unroll
+                    for (int u = 0; u < 2; u++) {
+                        int v = base + lane + (int)((ow >> (8 * (2 * h + u))) & 0xff);
+                        v -= v >= WR ? WR : 0;
+                        v -= v >= WR ? WR : 0;
+                        v -= v >= WR ? WR : 0;
+                        pr |= (unsigned)(v * kRhsPad) << (16 * u);
                     }
+                    words[2 * k4 + h] = pr;
                 }
             }
-            acc -= p[0] + p[1];
-            win[(r & A.mask) * kRhsPad + lane] = acc;
+#pragma unroll
+            for (int k = 0; k < W / 2; k++)
+                if (2 * k < wq) wi[lane * WIP + k] = words[k];
+        }
+        __syncwarp();  // every lane's copies and indices are visible to the warp
+        const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
+        for (int r = a1 - 1; r >= a0; r--) {
+            const int i = r - row0;
+            T acc = (T)S.b[i * kRhsPad + lane] * S.rd[i];
+            T p[2] = {T(0), T(0)};
+#pragma unroll
+            for (int k = 0; k < W / 2; k++) {
+                if (2 * k < wq) {
+                    const V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
+                    const unsigned w2 = wi[i * WIP + k];
+                    p[0] = fma(v2.x, win[(w2 & 0xffffu) + lane], p[0]);
+                    p[1] = fma(v2.y, win[(w2 >> 16) + lane], p[1]);
+                }
+            }
+            int slot = base + i;
+            slot -= slot >= WR ? WR : 0;
+            win[slot * kRhsPad + lane] = acc - (p[0] + p[1]);
         }
         __syncwarp();
         // x rows of this tile out (lane = row), for the rows this task stores
@@ -591,13 +624,14 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
             const int r = row0 + lane;
             if (r >= a0 && r < a1 && r >= t.st_lo && r < t.st_hi) {
                 const long long o = A.rev ? (long long)n - 1 - r : r;
-                const T *wr = win + (r & A.mask) * kRhsPad;
-#pragma unroll 8
-                for (int k = 0; k < 32; k++)
-                    if (k < A.nk) A.X[k * A.ldx + o] = (double)wr[k];
+                int slot = base + lane;
+                slot -= slot >= WR ? WR : 0;
+                const T *wr = win + slot * kRhsPad;
+                for (int k = 0; k < A.nk; k++) A.X[k * A.ldx + o] = (double)wr[k];
             }
         }
     }
+    cpa_wait<0>();
 }
 
 template <typename T, bool PRE>
@@ -617,11 +651,14 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
     A.ldx = ldx;
     A.rev = s->uplo == 'L';
     A.nk = nk;
-    A.mask = s->ch_win - 1;
+    A.wr = s->ch_reach + 32;
+    A.reach = s->ch_reach;
+    A.sw = s->ch_sw;
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     const int W = s->ch_width;
-    const size_t smem = sizeof(T) * ((size_t)s->ch_win * kRhsPad + 32 * (W + 2) + 32) + 4 * 32 * (W / 4 + 1) + 64;
+    const size_t smem = 2 * (size_t)rhs_stage_bytes(A.sw, sizeof(T)) + ((32 * (W / 2 + 1) * 4 + 15) & ~15) +
+                        sizeof(T) * (size_t)A.wr * kRhsPad;
     auto go = [&](auto kern) -> int {
         SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntasks, 32, smem, st>>>(A);
