@@ -272,27 +272,36 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
     const bool act = r >= t.lo && r < t.hi;
     double acc = act ? S.b[lane] * S.rd[lane] : 0.0;
     double p[4] = {0.0, 0.0, 0.0, 0.0};
-    unsigned ow[W / 4];
-#pragma unroll
-    for (int k = 0; k < W / 4; k++) ow[k] = 4 * k < wq ? S.o[32 * k + lane] : 0u;
     // Every slot stores its value into the lane's coefficient column (in-tile
     // columns at their row, the others into scratch row 32) and loads the
     // window value at its column, kept only for far columns (a select, so that
-    // a stale slot of the window cannot leak in): no branch.
+    // a stale slot of the window cannot leak in).  Groups of eight slots are
+    // branch-free (slots past the tile's width act as padding), so the loads of
+    // a group overlap.
 #pragma unroll
-    for (int k2 = 0; k2 < W / 2; k2++) {
-        if (2 * k2 < wq) {
-            const double2 v2 = S.v[32 * k2 + lane];
+    for (int g = 0; g < W / 8 + (W % 8 ? 1 : 0); g++) {
+        if (8 * g < wq) {
+            unsigned ow[2] = {0u, 0u};
+            double2 v2[4];
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int k = 2 * k2 + h;
-                const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
-                const double v = act ? (h ? v2.y : v2.x) : 0.0;
-                const bool in = d < 32;
-                coef[(in ? d : 32) * 32 + lane] = v;
-                const double wv = win[(row0 + d) & A.mask];
-                const double f = fma(v, wv, p[k & 3]);
-                p[k & 3] = in ? p[k & 3] : f;
+            for (int h = 0; h < 2; h++)
+                if (8 * g + 4 * h < W) ow[h] = S.o[32 * (2 * g + h) + lane];
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+                if (8 * g + 2 * h < W) v2[h] = S.v[32 * (4 * g + h) + lane];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int k = 8 * g + u;
+                if (k < W) {
+                    const bool live = act && k < wq;
+                    const int d = lane + (live ? (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff) : 0);
+                    const double v = live ? ((u & 1) ? v2[u >> 1].y : v2[u >> 1].x) : 0.0;
+                    const bool in = d < 32;
+                    coef[(in ? d : 32) * 32 + lane] = v;
+                    const double wv = win[(row0 + d) & A.mask];
+                    const double f = fma(v, wv, p[u & 3]);
+                    p[u & 3] = in ? p[u & 3] : f;
+                }
             }
         }
     }
@@ -323,12 +332,23 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
         win[r & A.mask] = acc;
         if (r >= t.st_lo && r < t.st_hi) A.x[A.rev ? A.n - 1 - r : r] = acc;
     }
-    // leave the coefficient column zero for the next tile (inactive lanes wrote zeros)
+    // leave the coefficient column zero for the next tile (inactive lanes and
+    // padding wrote zeros)
 #pragma unroll
-    for (int k = 0; k < W; k++) {
-        if (k < wq) {
-            const int d = lane + ((ow[k >> 2] >> (8 * (k & 3))) & 0xff);
-            if (d < 32) coef[d * 32 + lane] = 0.0;
+    for (int g = 0; g < W / 8 + (W % 8 ? 1 : 0); g++) {
+        if (8 * g < wq) {
+            unsigned ow[2] = {0u, 0u};
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (8 * g + 4 * h < W) ow[h] = S.o[32 * (2 * g + h) + lane];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int k = 8 * g + u;
+                if (k < W) {
+                    const int d = lane + (k < wq ? (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff) : 0);
+                    if (d < 32) coef[d * 32 + lane] = 0.0;
+                }
+            }
         }
     }
     __syncwarp();
@@ -595,9 +615,10 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
                     words[2 * k4 + h] = pr;
                 }
             }
+            // every word, so that the slots past the tile's width (own row,
+            // weight zero below) index the window
 #pragma unroll
-            for (int k = 0; k < W / 2; k++)
-                if (2 * k < wq) wi[lane * WIP + k] = words[k];
+            for (int k = 0; k < W / 2; k++) wi[lane * WIP + k] = words[k];
         }
         __syncwarp();  // every lane's copies and indices are visible to the warp
         const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
@@ -605,13 +626,22 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
             const int i = r - row0;
             T acc = (T)S.b[i * kRhsPad + lane] * S.rd[i];
             T p[2] = {T(0), T(0)};
+            // groups of four slot pairs, branch-free inside (pairs past the
+            // tile's width get weight zero)
 #pragma unroll
-            for (int k = 0; k < W / 2; k++) {
-                if (2 * k < wq) {
-                    const V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
-                    const unsigned w2 = wi[i * WIP + k];
-                    p[0] = fma(v2.x, win[(w2 & 0xffffu) + lane], p[0]);
-                    p[1] = fma(v2.y, win[(w2 >> 16) + lane], p[1]);
+            for (int g = 0; g < (W + 7) / 8; g++) {
+                if (8 * g < wq) {
+#pragma unroll
+                    for (int h = 0; h < 4; h++) {
+                        const int k = 4 * g + h;
+                        if (2 * k < W) {
+                            V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
+                            if (2 * k >= wq) v2.x = v2.y = T(0);
+                            const unsigned w2 = wi[i * WIP + k];
+                            p[0] = fma(v2.x, win[(w2 & 0xffffu) + lane], p[0]);
+                            p[1] = fma(v2.y, win[(w2 >> 16) + lane], p[1]);
+                        }
+                    }
                 }
             }
             int slot = base + i;
@@ -757,6 +787,8 @@ void chain_release(spk_system *s) {
 
 }  // namespace
 
+int chain_occupancy(spk_system *s, int *occ);
+
 // Build the chain layout, the chains' spikes and the two task lists; leaves
 // chain_ok = 0 (the partition-based solve) when truncation is off, the layout
 // does not apply (column distance > 128, more than 64 off-diagonals in a row),
@@ -791,7 +823,7 @@ int chain_prepare(spk_system *s) {
     if (reach < 1 || reach > 128 || wmax > 64 || tot >= 2147483647ll) return SPK_OK;
     ptr[ntiles] = (int)tot;
     s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : (wmax <= 32 ? 32 : 64)));
-    s->ch_sw = wmax;
+    s->ch_sw = (wmax + 7) & ~7;  // stages hold whole groups of eight slots
     s->ch_reach = reach;
     int win = 64;
     while (win < reach + 32) win <<= 1;
@@ -803,8 +835,13 @@ int chain_prepare(spk_system *s) {
                                                                  s->ch_ptr.p, s->ch_val.p, s->ch_off.p);
     SPK_CUDA(cudaGetLastError());
 
-    // chain length: about eight chains per SM, at least 1024 rows; doubled until valid
-    long long len = 32ll * ((n / (148 * 8) + 31) / 32);
+    // chain length: as many chains as the solve kernel keeps resident on the
+    // GPU at once (one wave), at least 1024 rows; doubled until valid
+    int dev = 0, sms = 148, occ = 8;
+    SPK_CUDA(cudaGetDevice(&dev));
+    SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SPK_TRY(chain_occupancy(s, &occ));
+    long long len = 32ll * ((n / (sms * (long long)std::max(occ, 1)) + 31) / 32);
     len = std::max<long long>(len, 1024);
     if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
     // at most three doublings, and never fewer than 8 chains
@@ -846,6 +883,23 @@ int chain_prepare(spk_system *s) {
     }
     chain_release(s);
     return SPK_OK;
+}
+
+// Resident blocks per SM of the phase-1 solve kernel (its shared memory bounds it).
+int chain_occupancy(spk_system *s, int *occ) {
+    const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (33 * 32 + s->ch_win);
+    auto q = [&](auto kern) -> int {
+        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
+        return SPK_OK;
+    };
+    switch (s->ch_width) {
+        case 4: return q(k_chain_solve<false, 4>);
+        case 8: return q(k_chain_solve<false, 8>);
+        case 16: return q(k_chain_solve<false, 16>);
+        case 32: return q(k_chain_solve<false, 32>);
+        default: return q(k_chain_solve<false, 64>);
+    }
 }
 
 // One solve of host arrays b and x through the chain path with the copies
