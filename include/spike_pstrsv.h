@@ -233,6 +233,19 @@ int spk_debug_array(const spk_system *s, const char *name, void *dst, long long 
                     long long *count, char *type);
 long long spk_debug_scalar(const spk_system *s, const char *name);
 
+/* One phase of the chain solve over U rows [row_lo, row_hi) (U order: for
+ * uplo 'L', U row r is caller row n-1-r), on device arrays b and x in the
+ * caller's order, on `stream`.  No reference counterpart: it is the building
+ * block of a solve whose rows are sharded over several GPUs.  Phase 1 solves
+ * every chain that starts in the range with zero coupling and stores its final
+ * rows; phase 4 re-solves the coupled rows of every chain that ends in the range,
+ * reading x at the `chain_reach` rows below each chain.  A shard therefore runs
+ * phase 1, receives x of the first chain_reach rows of the next shard (final
+ * after that shard's phase 1), then runs phase 4.  Chain bounds:
+ * spk_debug_array "chain_tasks1" / "chain_tasks4" (lo, hi, st_lo, st_hi per
+ * task).  SPK_ERR_STATE unless spk_debug_scalar(s, "chain") == 1. */
+int spk_chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *b, double *x, void *stream);
+
 /* Test hook (no reference counterpart): spk_debug_set(s, "fail_waits", 1) makes
  * every solve kernel of s report a failed bounded wait at entry, before it
  * issues any copy, until the failure has been reported once (SPK_ERR_TIMEOUT

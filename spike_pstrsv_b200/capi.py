@@ -58,6 +58,7 @@ def lib() -> ctypes.CDLL:
         L.spk_debug_scalar.restype = ctypes.c_longlong
         L.spk_debug_scalar.argtypes = [vp, ctypes.c_char_p]
         L.spk_debug_set.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
+        L.spk_chain_phase.argtypes = [vp, i, i, i, vp, vp, vp]
         L.spk_legacy_system.restype = vp
         L.spk_set_truncation.argtypes = [vp, d]
         L.spk_check.argtypes = [vp]
@@ -210,6 +211,7 @@ class System:
         _check(lib().spk_create(ctypes.byref(h)))
         self.h = h
         self.n = 0
+        self.uplo = "U"
 
     def close(self):
         if self.h:
@@ -231,6 +233,7 @@ class System:
                                  _arr(ja, np.int32, keep), int(n), int(nparts), _uplo(uplo),
                                  int(flb), st, en))
         self.n = int(n)
+        self.uplo = uplo.upper() if isinstance(uplo, str) else chr(uplo[0]).upper()
         return self
 
     def set_truncation(self, tau: float) -> "System":
@@ -299,6 +302,12 @@ class System:
 
     def scalar(self, name: str) -> int:
         return int(lib().spk_debug_scalar(self.h, name.encode()))
+
+    def chain_phase(self, phase: int, row_lo: int, row_hi: int, b_ptr: int, x_ptr: int, stream: int = 0) -> None:
+        """One phase (1 or 4) of the chain solve over U rows [row_lo, row_hi), on
+        device pointers (spk_chain_phase)."""
+        _check(lib().spk_chain_phase(self.h, int(phase), int(row_lo), int(row_hi), ctypes.c_void_p(b_ptr),
+                                     ctypes.c_void_p(x_ptr), ctypes.c_void_p(stream)))
 
     def debug_set(self, name: str, value: int) -> "System":
         """Test hooks (spk_debug_set): "fail_waits" makes the solve kernels report a

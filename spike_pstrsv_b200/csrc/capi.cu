@@ -1,6 +1,7 @@
 // Exported C ABI: the reference's five entry points and profiler globals
 // (single resident system, as the reference's static arrays), and the
 // handle-based spk_* extension.
+#include <algorithm>
 #include <cstdarg>
 #include <ctime>
 #include <cstdint>
@@ -527,6 +528,26 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     return -1;
 }
 
+int spk_chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *b, double *x, void *stream) {
+    if (!s || !b || !x) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!s->built || !s->chain_ok) {
+        set_error(SPK_ERR_STATE, "spk_chain_phase needs a system solved by chains (default truncation, banded rows)");
+        return SPK_ERR_STATE;
+    }
+    if ((phase != 1 && phase != 4) || row_lo < 0 || row_hi > s->n || row_lo > row_hi) {
+        set_error(SPK_ERR_ARG, "invalid chain phase %d or row range [%d, %d)", phase, row_lo, row_hi);
+        return SPK_ERR_ARG;
+    }
+    if (!is_device_pointer(b) || !is_device_pointer(x)) {
+        set_error(SPK_ERR_ARG, "spk_chain_phase takes device arrays");
+        return SPK_ERR_ARG;
+    }
+    return chain_phase(s, phase, row_lo, row_hi, b, x, (cudaStream_t)stream);
+}
+
 int spk_debug_set(spk_system *s, const char *name, long long value) {
     if (!s || !name) {
         set_error(SPK_ERR_ARG, "null argument");
@@ -620,6 +641,14 @@ int spk_debug_array(const spk_system *s, const char *name, void *dst, long long 
     else if (!strcmp(name, "U_ia")) { src = s->uia.p; cnt = n + 1; }
     else if (!strcmp(name, "U_ja")) { src = s->uja.p; cnt = s->nnz; }
     else if (!strcmp(name, "U_a")) { src = s->ua.p; cnt = s->nnz; ty = 'd'; }
+    else if (!strcmp(name, "chain_tasks1") || !strcmp(name, "chain_tasks4")) {
+        // (lo, hi, st_lo, st_hi) per task, U order, host copies
+        const std::vector<ChainTask> &v = name[11] == '1' ? s->h_ctasks1 : s->h_ctasks4;
+        *count = 4LL * (long long)v.size();
+        *type = 'i';
+        if (dst) memcpy(dst, v.data(), sizeof(int) * (size_t)std::min<long long>(cap, *count));
+        return SPK_OK;
+    }
     else {
         set_error(SPK_ERR_ARG, "unknown array '%s'", name);
         return SPK_ERR_ARG;

@@ -1002,6 +1002,17 @@ int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long 
     return SPK_OK;
 }
 
+// The tasks of one phase whose chains lie in U rows [row_lo, row_hi): phase 1
+// tasks start at their chain's first row, phase 4 tasks end at its last row.
+int chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *b, double *x, cudaStream_t st) {
+    const std::vector<ChainTask> &v = phase == 1 ? s->h_ctasks1 : s->h_ctasks4;
+    int i0 = 0, i1 = 0;
+    for (i0 = 0; i0 < (int)v.size() && (phase == 1 ? v[i0].lo : v[i0].hi - 1) < row_lo; i0++) {}
+    for (i1 = i0; i1 < (int)v.size() && (phase == 1 ? v[i1].hi : v[i1].hi) <= row_hi; i1++) {}
+    if (phase == 1) return launch_chain<false>(s, s->d_ctasks1.p + i0, i1 - i0, b, x, st);
+    return launch_chain<true>(s, s->d_ctasks4.p + i0, i1 - i0, b, x, st);
+}
+
 // One solve through the chain path: phase 1 then phase 4 on stream st.
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring) {
     SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p, s->nctasks1, b, x, st));
