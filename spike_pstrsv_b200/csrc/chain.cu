@@ -267,17 +267,16 @@ __device__ __forceinline__ void stage_tile(const ChainArgs &A, const ChainStage 
 
 template <int W>
 __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage &S, int wq, int j,
-                                           const ChainTask &t, double *coef, double *win, int lane) {
+                                           const ChainTask &t, double *coef, unsigned *msk, double *win, int lane) {
     const int row0 = 32 * j, r = row0 + lane;
     const bool act = r >= t.lo && r < t.hi;
     double acc = act ? S.b[lane] * S.rd[lane] : 0.0;
     double p[4] = {0.0, 0.0, 0.0, 0.0};
-    // Every slot stores its value into the lane's coefficient column (in-tile
-    // columns at their row, the others into scratch row 32) and loads the
-    // window value at its column, kept only for far columns (a select, so that
-    // a stale slot of the window cannot leak in).  Groups of eight slots are
-    // branch-free (slots past the tile's width act as padding), so the loads of
-    // a group overlap.
+    unsigned mask = 0u;  // bit i: this row has the in-tile column row0 + i
+    // In-tile columns go into the lane's coefficient column (and its mask),
+    // far columns multiply the window value at their row.  Groups of eight
+    // slots are branch-free (slots past the tile's width are dead), so the
+    // loads of a group overlap.
 #pragma unroll
     for (int g = 0; g < W / 8 + (W % 8 ? 1 : 0); g++) {
         if (8 * g < wq) {
@@ -293,32 +292,37 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
             for (int u = 0; u < 8; u++) {
                 const int k = 8 * g + u;
                 if (k < W) {
-                    const bool live = act && k < wq;
-                    const int d = lane + (live ? (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff) : 0);
-                    const double v = live ? ((u & 1) ? v2[u >> 1].y : v2[u >> 1].x) : 0.0;
-                    const bool in = d < 32;
-                    coef[(in ? d : 32) * 32 + lane] = v;
-                    const double wv = win[(row0 + d) & A.mask];
-                    const double f = fma(v, wv, p[u & 3]);
-                    p[u & 3] = in ? p[u & 3] : f;
+                    const int o = (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff);
+                    const bool live = act && k < wq && o > 0;  // offset 0: padding
+                    const int d = lane + o;
+                    const double v = (u & 1) ? v2[u >> 1].y : v2[u >> 1].x;
+                    if (live && d < 32) {
+                        coef[d * 32 + lane] = v;
+                        mask |= 1u << d;
+                    }
+                    if (live && d >= 32) p[u & 3] = fma(v, win[(row0 + d) & A.mask], p[u & 3]);
                 }
             }
         }
     }
     acc -= (p[0] + p[1]) + (p[2] + p[3]);
-    __syncwarp();  // the block coefficients below read other lanes' columns
+    msk[lane] = mask;
+    __syncwarp();  // the block coefficients and masks below are other lanes'
     // In-tile triangle, bottom-up, four rows per step: the four accumulators are
     // broadcast together, every lane resolves the block's four unknowns from the
-    // block's six coefficients (uniform loads) and applies all four columns.  A
-    // lane's coefficients at or below its own row are zero, so lanes inside the
-    // block come out with their final values too.
+    // block's six coefficients and applies all four columns.  Coefficients are
+    // read under the masks (a column no row of this tile set holds an older
+    // tile's value and is never used), so nothing is cleared between tiles.
 #pragma unroll
     for (int i = 31; i >= 3; i -= 4) {
-        const double c0 = coef[i * 32 + lane], c1 = coef[(i - 1) * 32 + lane];
-        const double c2 = coef[(i - 2) * 32 + lane], c3 = coef[(i - 3) * 32 + lane];
-        const double u10 = coef[i * 32 + i - 1];
-        const double u20 = coef[i * 32 + i - 2], u21 = coef[(i - 1) * 32 + i - 2];
-        const double u30 = coef[i * 32 + i - 3], u31 = coef[(i - 1) * 32 + i - 3], u32 = coef[(i - 2) * 32 + i - 3];
+        const uint4 mq = *reinterpret_cast<const uint4 *>(msk + i - 3);  // rows i-3 .. i
+        auto cf = [&](bool has, int col, int row) { return has ? coef[col * 32 + row] : 0.0; };
+        const double c0 = cf((mask >> i) & 1u, i, lane), c1 = cf((mask >> (i - 1)) & 1u, i - 1, lane);
+        const double c2 = cf((mask >> (i - 2)) & 1u, i - 2, lane), c3 = cf((mask >> (i - 3)) & 1u, i - 3, lane);
+        const double u10 = cf((mq.z >> i) & 1u, i, i - 1);
+        const double u20 = cf((mq.y >> i) & 1u, i, i - 2), u21 = cf((mq.y >> (i - 1)) & 1u, i - 1, i - 2);
+        const double u30 = cf((mq.x >> i) & 1u, i, i - 3), u31 = cf((mq.x >> (i - 1)) & 1u, i - 1, i - 3);
+        const double u32 = cf((mq.x >> (i - 2)) & 1u, i - 2, i - 3);
         const double b0 = __shfl_sync(kFull, acc, i), b1 = __shfl_sync(kFull, acc, i - 1);
         const double b2 = __shfl_sync(kFull, acc, i - 2), b3 = __shfl_sync(kFull, acc, i - 3);
         const double a1 = fma(-u10, b0, b1);
@@ -327,31 +331,11 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
         const double t01 = fma(-c1, a1, fma(-c0, b0, acc));
         acc = fma(-c3, a3, fma(-c2, a2, t01));
     }
-    __syncwarp();  // block coefficients read before the columns are cleared
     if (act) {
         win[r & A.mask] = acc;
         if (r >= t.st_lo && r < t.st_hi) A.x[A.rev ? A.n - 1 - r : r] = acc;
     }
-    // leave the coefficient column zero for the next tile (inactive lanes and
-    // padding wrote zeros)
-#pragma unroll
-    for (int g = 0; g < W / 8 + (W % 8 ? 1 : 0); g++) {
-        if (8 * g < wq) {
-            unsigned ow[2] = {0u, 0u};
-#pragma unroll
-            for (int h = 0; h < 2; h++)
-                if (8 * g + 4 * h < W) ow[h] = S.o[32 * (2 * g + h) + lane];
-#pragma unroll
-            for (int u = 0; u < 8; u++) {
-                const int k = 8 * g + u;
-                if (k < W) {
-                    const int d = lane + (k < wq ? (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff) : 0);
-                    if (d < 32) coef[d * 32 + lane] = 0.0;
-                }
-            }
-        }
-    }
-    __syncwarp();
+    __syncwarp();  // window rows and coefficient reads done before the next tile
 }
 
 // PRE: phase 4 (the window starts with x of rows [hi, hi + window)); else
@@ -362,16 +346,15 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     ChainStage stg[kChainStages];
 #pragma unroll
     for (int s = 0; s < kChainStages; s++) stg[s] = chain_stage(smc, s, A.sw);
-    double *coef = (double *)(smc + kChainStages * chain_stage_bytes(A.sw));  // [33 rows][32 lanes]; row 32: scratch
-    double *win = coef + 33 * 32;                                             // [mask + 1]
+    double *coef = (double *)(smc + kChainStages * chain_stage_bytes(A.sw));  // [32 columns][32 lanes]
+    unsigned *msk = (unsigned *)(coef + 32 * 32);                             // [32] in-tile column masks
+    double *win = coef + 32 * 32 + 16;                                        // [mask + 1]
     const int lane = threadIdx.x;
     if (A.fail_entry) {
         if (lane == 0) atomicExch(A.err, 1);
         return;
     }
     const ChainTask t = A.tasks[blockIdx.x];
-#pragma unroll
-    for (int i = 0; i < 33; i++) coef[i * 32 + lane] = 0.0;
     for (int k = lane; k <= A.mask; k += 32) {
         const int r = t.hi + k;
         double v = 0.0;
@@ -421,7 +404,7 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
                 }
                 cpa_commit();
                 cpa_wait<kChainStages - 1>();  // this tile's copies have landed (own lane's)
-                solve_tile<W>(A, stg[s], wq_st[s], j, t, coef, win, lane);
+                solve_tile<W>(A, stg[s], wq_st[s], j, t, coef, msk, win, lane);
             }
         }
     }
@@ -447,7 +430,7 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     auto go = [&](auto kern) -> int {
-        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (33 * 32 + s->ch_win);
+        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
         SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntasks, 32, smem, st>>>(A);
         SPK_CUDA(cudaGetLastError());
@@ -841,7 +824,8 @@ int chain_prepare(spk_system *s) {
     SPK_CUDA(cudaGetDevice(&dev));
     SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     SPK_TRY(chain_occupancy(s, &occ));
-    long long len = 32ll * ((n / (sms * (long long)std::max(occ, 1)) + 31) / 32);
+    // (seven per SM at most: with more, phase 1 gains nothing and phase 4 grows)
+    long long len = 32ll * ((n / (sms * (long long)std::min(std::max(occ, 1), 7)) + 31) / 32);
     len = std::max<long long>(len, 1024);
     if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
     // at most three doublings, and never fewer than 8 chains
@@ -887,7 +871,7 @@ int chain_prepare(spk_system *s) {
 
 // Resident blocks per SM of the phase-1 solve kernel (its shared memory bounds it).
 int chain_occupancy(spk_system *s, int *occ) {
-    const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (33 * 32 + s->ch_win);
+    const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
     auto q = [&](auto kern) -> int {
         SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));

@@ -2239,7 +2239,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     const size_t col_bytes = ((size_t)32 * n * sizeof(double) + 255) / 256 * 256;
     char *work_p = nullptr;
     double *rbuf_p = nullptr, *dbuf_p = nullptr;
-    if (mode == 1 && !s->chain_ok) {
+    if (mode == 1) {
         SPK_TRY(ensure_fp32(s));
         SPK_TRY(ensure_reach(s));
     }
@@ -2273,9 +2273,16 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     SPK_CUDA(cudaGetDevice(&dev));
     SPK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const bool wide_ok = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms;
-    if (s->chain_ok) {
+    int dev0 = 0, sms0 = 148;
+    SPK_CUDA(cudaGetDevice(&dev0));
+    SPK_CUDA(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
+    const bool part_wide = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms0;
+    const char *cb = getenv("SPK_CHAIN_BATCH");  // 1: always the chain kernels, 0: never
+    const bool use_chain = s->chain_ok && (cb ? cb[0] == '1' : !part_wide);
+    if (use_chain) {
         // the chain tasks fill the GPU whatever the partition count: every group
-        // of up to 32 columns is one right-hand-side-parallel chain solve
+        // of up to 32 columns is one right-hand-side-parallel chain solve (used
+        // when the partitions alone give too few tasks to fill the GPU)
         for (int g = 0; g < nrhs;) {
             const int K = std::min(nrhs - g, 32);
             const double *Bg = B + g * ldb;

@@ -135,12 +135,13 @@ def test_pipelined_host_solve(monkeypatch, chunks):
 
 @pytest.mark.parametrize("uplo", ["L", "U"])
 @pytest.mark.parametrize("nrhs", [1, 5, 32, 40])
-def test_chain_batched_matches_substitution(uplo, nrhs):
+def test_chain_batched_matches_substitution(monkeypatch, uplo, nrhs):
     """Batched solves through the right-hand-side-parallel chain kernel (lane =
     right-hand side): FP64 against the sequential substitution of every column,
     FP32 + FP64 refinement to scaled residual 1e-12."""
     import torch
 
+    monkeypatch.setenv("SPK_CHAIN_BATCH", "1")  # the chain kernels whatever the partition count
     L = synth.banded_lower(120000, seed=12)
     A = L if uplo == "L" else synth.transpose(L)
     Xt, B = synth.make_rhs(A, seed=12, nrhs=nrhs)
