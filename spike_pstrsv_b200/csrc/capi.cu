@@ -509,6 +509,8 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "chain_rows_phase1")) return s->ch_rows1;
     if (!strcmp(name, "chain_rows_phase4")) return s->ch_rows4;
     if (!strcmp(name, "chain_tasks_phase4")) return s->nctasks4;
+    if (!strcmp(name, "chain_batch_rows")) return s->chb_len;
+    if (!strcmp(name, "chain_batch_tasks_phase4")) return s->nbtasks1 ? s->nbtasks4 : s->nctasks4;
     if (!strcmp(name, "chain_bytes")) return (long long)(s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes());
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
     if (!strcmp(name, "kept_reduced_rows")) return s->nkept;

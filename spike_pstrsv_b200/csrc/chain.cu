@@ -593,7 +593,7 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
                         v -= v >= WR ? WR : 0;
                         v -= v >= WR ? WR : 0;
                         v -= v >= WR ? WR : 0;
-                        pr |= (unsigned)(v * kRhsPad) << (16 * u);
+                        pr |= (unsigned)(v * kRhsPad * (int)sizeof(T)) << (16 * u);  // byte offset
                     }
                     words[2 * k4 + h] = pr;
                 }
@@ -602,15 +602,23 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
             // weight zero below) index the window
 #pragma unroll
             for (int k = 0; k < W / 2; k++) wi[lane * WIP + k] = words[k];
+            // a half-filled group of eight slots: zero weights for its second half
+            if (wq & 4) {
+                S.v[64 * (wq >> 1) + 2 * lane] = T(0);
+                S.v[64 * (wq >> 1) + 2 * lane + 1] = T(0);
+                S.v[64 * ((wq >> 1) + 1) + 2 * lane] = T(0);
+                S.v[64 * ((wq >> 1) + 1) + 2 * lane + 1] = T(0);
+            }
         }
         __syncwarp();  // every lane's copies and indices are visible to the warp
         const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
+        const char *wl = (const char *)(win + lane);  // this lane's column of the window
         for (int r = a1 - 1; r >= a0; r--) {
             const int i = r - row0;
             T acc = (T)S.b[i * kRhsPad + lane] * S.rd[i];
             T p[2] = {T(0), T(0)};
-            // groups of four slot pairs, branch-free inside (pairs past the
-            // tile's width get weight zero)
+            // groups of four slot pairs, branch-free inside (the second half of a
+            // half-filled group has weight zero)
 #pragma unroll
             for (int g = 0; g < (W + 7) / 8; g++) {
                 if (8 * g < wq) {
@@ -618,11 +626,10 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
                     for (int h = 0; h < 4; h++) {
                         const int k = 4 * g + h;
                         if (2 * k < W) {
-                            V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
-                            if (2 * k >= wq) v2.x = v2.y = T(0);
+                            const V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
                             const unsigned w2 = wi[i * WIP + k];
-                            p[0] = fma(v2.x, win[(w2 & 0xffffu) + lane], p[0]);
-                            p[1] = fma(v2.y, win[(w2 >> 16) + lane], p[1]);
+                            p[0] = fma(v2.x, *reinterpret_cast<const T *>(wl + (w2 & 0xffffu)), p[0]);
+                            p[1] = fma(v2.y, *reinterpret_cast<const T *>(wl + (w2 >> 16)), p[1]);
                         }
                     }
                 }
@@ -645,6 +652,12 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
         }
     }
     cpa_wait<0>();
+}
+
+size_t rhs_smem_bytes(const spk_system *s, int tsize) {
+    const int W = s->ch_width;
+    return 2 * (size_t)rhs_stage_bytes(s->ch_sw, tsize) + ((32 * (W / 2 + 1) * 4 + 15) & ~15) +
+           (size_t)tsize * (s->ch_reach + 32) * kRhsPad;
 }
 
 template <typename T, bool PRE>
@@ -670,8 +683,7 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     const int W = s->ch_width;
-    const size_t smem = 2 * (size_t)rhs_stage_bytes(A.sw, sizeof(T)) + ((32 * (W / 2 + 1) * 4 + 15) & ~15) +
-                        sizeof(T) * (size_t)A.wr * kRhsPad;
+    const size_t smem = rhs_smem_bytes(s, sizeof(T));
     auto go = [&](auto kern) -> int {
         SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<ntasks, 32, smem, st>>>(A);
@@ -760,6 +772,10 @@ void chain_release(spk_system *s) {
     s->ch_ptr.release();
     s->d_ctasks1.release();
     s->d_ctasks4.release();
+    s->d_btasks1.release();
+    s->d_btasks4.release();
+    s->nbtasks1 = s->nbtasks4 = 0;
+    s->chb_len = 0;
     s->h_ctasks1.clear();
     s->h_ctasks4.clear();
     s->nctasks1 = s->nctasks4 = 0;
@@ -771,6 +787,8 @@ void chain_release(spk_system *s) {
 }  // namespace
 
 int chain_occupancy(spk_system *s, int *occ);
+int chain_rhs_occupancy(spk_system *s, int *occ);
+int build_plan(spk_system *s, long long len, int reach, bool batch);
 
 // Build the chain layout, the chains' spikes and the two task lists; leaves
 // chain_ok = 0 (the partition-based solve) when truncation is off, the layout
@@ -828,9 +846,30 @@ int chain_prepare(spk_system *s) {
     long long len = 32ll * ((n / (sms * (long long)std::min(std::max(occ, 1), 7)) + 31) / 32);
     len = std::max<long long>(len, 1024);
     if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
-    // at most three doublings, and never fewer than 8 chains
+    SPK_TRY(build_plan(s, len, reach, false));
+    if (!s->chain_ok) return SPK_OK;
+    // the batched kernel keeps fewer tasks resident (a wider window): its own
+    // chains, as many as it keeps resident
+    int occb = 4;
+    SPK_TRY(chain_rhs_occupancy(s, &occb));
+    long long lenb = 32ll * ((n / (sms * (long long)std::max(occb, 1)) + 31) / 32);
+    lenb = std::max<long long>(lenb, s->ch_len);
+    if (const char *e = getenv("SPK_CHAIN_BATCH_ROWS")) lenb = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
+    SPK_TRY(build_plan(s, lenb, reach, true));
+    return SPK_OK;
+}
+
+// Chains of `len` rows (doubled up to three times until every chain keeps its
+// first `reach` rows, never fewer than 8 chains): their spikes, the two task
+// lists (row order: the pipelined and sharded solves launch them by row range).
+// batch = false: the plain solve's plan (sets chain_ok, or releases everything
+// when no length is valid); true: the batched kernel's plan (falls back to the
+// plain plan's tasks when no length is valid).
+int build_plan(spk_system *s, long long len, int reach, bool batch) {
+    const int n = s->n;
     const long long max_len = std::min<long long>(8 * len, std::max<long long>(len, 32ll * ((n / 8 + 31) / 32)));
     for (; len <= max_len; len *= 2) {
+        if (batch && len == s->ch_len) break;  // the same chains as the plain solve
         std::vector<int2> chains;
         for (long long a = 0; a < n; a += len)
             chains.push_back(make_int2((int)a, (int)std::min<long long>(a + len, n)));
@@ -851,7 +890,14 @@ int chain_prepare(spk_system *s) {
                 rows4 += q - f;
             }
         }
-        // both lists stay in row order: the pipelined solve launches them chunk by chunk
+        if (batch) {
+            SPK_TRY(upload_vec(s->d_btasks1, t1));
+            SPK_TRY(upload_vec(s->d_btasks4, t4));
+            s->nbtasks1 = (int)t1.size();
+            s->nbtasks4 = (int)t4.size();
+            s->chb_len = (int)len;
+            return SPK_OK;
+        }
         s->h_ctasks1 = t1;
         s->h_ctasks4 = t4;
         SPK_TRY(upload_vec(s->d_ctasks1, t1));
@@ -863,6 +909,13 @@ int chain_prepare(spk_system *s) {
         s->ch_count = (int)chains.size();
         s->ch_len = (int)len;
         s->chain_ok = 1;
+        return SPK_OK;
+    }
+    if (batch) {
+        s->d_btasks1.release();
+        s->d_btasks4.release();
+        s->nbtasks1 = s->nbtasks4 = 0;
+        s->chb_len = s->ch_len;  // the batched kernel takes the plain solve's tasks
         return SPK_OK;
     }
     chain_release(s);
@@ -883,6 +936,24 @@ int chain_occupancy(spk_system *s, int *occ) {
         case 16: return q(k_chain_solve<false, 16>);
         case 32: return q(k_chain_solve<false, 32>);
         default: return q(k_chain_solve<false, 64>);
+    }
+}
+
+// Resident blocks per SM of the batched (FP64) chain kernel.
+int chain_rhs_occupancy(spk_system *s, int *occ) {
+    const int W = s->ch_width;
+    const size_t smem = rhs_smem_bytes(s, sizeof(double));
+    auto q = [&](auto kern) -> int {
+        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
+        return SPK_OK;
+    };
+    switch (W) {
+        case 4: return q(k_chain_rhs<double, 4, false>);
+        case 8: return q(k_chain_rhs<double, 8, false>);
+        case 16: return q(k_chain_rhs<double, 16, false>);
+        case 32: return q(k_chain_rhs<double, 32, false>);
+        default: return q(k_chain_rhs<double, 64, false>);
     }
 }
 
@@ -975,13 +1046,16 @@ int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long 
         set_error(SPK_ERR_ARG, "chain batch of %d columns (1..32)", nk);
         return SPK_ERR_ARG;
     }
+    const bool own = s->nbtasks1 > 0;  // the batched kernel's own chains
+    const ChainTask *t1 = own ? s->d_btasks1.p : s->d_ctasks1.p, *t4 = own ? s->d_btasks4.p : s->d_ctasks4.p;
+    const int n1 = own ? s->nbtasks1 : s->nctasks1, n4 = own ? s->nbtasks4 : s->nctasks4;
     if (fp32) {
         SPK_TRY(chain_fp32(s));
-        SPK_TRY((launch_chain_rhs<float, false>(s, s->d_ctasks1.p, s->nctasks1, nk, B, ldb, X, ldx, st)));
-        SPK_TRY((launch_chain_rhs<float, true>(s, s->d_ctasks4.p, s->nctasks4, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<float, false>(s, t1, n1, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<float, true>(s, t4, n4, nk, B, ldb, X, ldx, st)));
     } else {
-        SPK_TRY((launch_chain_rhs<double, false>(s, s->d_ctasks1.p, s->nctasks1, nk, B, ldb, X, ldx, st)));
-        SPK_TRY((launch_chain_rhs<double, true>(s, s->d_ctasks4.p, s->nctasks4, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<double, false>(s, t1, n1, nk, B, ldb, X, ldx, st)));
+        SPK_TRY((launch_chain_rhs<double, true>(s, t4, n4, nk, B, ldb, X, ldx, st)));
     }
     return SPK_OK;
 }

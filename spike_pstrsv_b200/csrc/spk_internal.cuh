@@ -159,6 +159,8 @@ struct spk_system {
     spk::DBuf<unsigned char> ch_off;   // column offsets c - r (8 bits)
     spk::DBuf<int> ch_ptr;             // first slot of each 32-row tile
     spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;
+    spk::DBuf<spk::ChainTask> d_btasks1, d_btasks4;  // the batched kernel's own chains (longer)
+    int nbtasks1 = 0, nbtasks4 = 0, chb_len = 0;
     int nctasks1 = 0, nctasks4 = 0;
     long long ch_rows1 = 0, ch_rows4 = 0;
     std::vector<spk::ChainTask> h_ctasks1, h_ctasks4;
