@@ -45,7 +45,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     tmp = LIB + ".tmp"
-    cmd = [nvcc()] + ARCH + FLAGS + ["-I" + os.path.join(ROOT, "include"), "-o", tmp] + sources()
+    extra = os.environ.get("SPK_NVCC_EXTRA", "").split()  # e.g. -DSPK_DEVICE_CHECKS (checked build)
+    cmd = [nvcc()] + ARCH + FLAGS + extra + ["-I" + os.path.join(ROOT, "include"), "-o", tmp] + sources()
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -98,8 +98,26 @@ int make_system(spk_system **out) {
     return SPK_OK;
 }
 
+// SPK_DEBUG_SYNC=1: report the first CUDA error of the teardown steps on stderr
+static bool debug_sync() {
+    static const bool on = [] {
+        const char *e = getenv("SPK_DEBUG_SYNC");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+static void debug_check(const char *where, const spk_system *s = nullptr) {
+    if (!debug_sync()) return;
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+        fprintf(stderr, "spike_pstrsv debug: %s (n=%d chain=%d): %s\n", where, s ? s->n : -1, s ? s->chain_ok : -1,
+                cudaGetErrorString(e));
+}
+
 void destroy_system(spk_system *s) {
     if (!s) return;
+    debug_check("before teardown", s);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto &set : s->ev)
         for (auto &e : set)
@@ -109,7 +127,9 @@ void destroy_system(spk_system *s) {
     for (cudaStream_t q : s->pipe_st) cudaStreamDestroy(q);
     if (s->st_in) cudaStreamDestroy(s->st_in);
     if (s->st_out) cudaStreamDestroy(s->st_out);
+    debug_check("after stream teardown", s);
     delete s;
+    debug_check("after buffer release");
 }
 
 void export_partitions(const spk_system *s) {
@@ -339,7 +359,9 @@ int spk_preproc(spk_system *s, const double *a, const int *ia, const int *ja, in
         return SPK_ERR_ARG;
     }
     int on_dev = is_device_pointer(a) && is_device_pointer(ia) && is_device_pointer(ja);
-    return preprocess(s, a, ia, ja, n, nparts, uplo, flb, starts, ends, on_dev, nullptr);
+    const int rc = preprocess(s, a, ia, ja, n, nparts, uplo, flb, starts, ends, on_dev, nullptr);
+    debug_check("after preprocessing", s);
+    return rc;
 }
 
 int spk_solve_device(spk_system *s, const double *b, double *x, void *stream) {
@@ -374,13 +396,19 @@ int spk_solve(spk_system *s, const double *b, double *x) {
     }
     if (!bd && !xd && s->chain_ok) {
         SPK_TRY(chain_solve_host(s, b, x, s->stage_b.p, s->stage_x.p));
-        return check_device_error(s);
+        debug_check("after the pipelined solve", s);
+        const int rc = check_device_error(s);
+        debug_check("after the error word", s);
+        return rc;
     }
     if (!bd) SPK_CUDA(cudaMemcpyAsync(s->stage_b.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, s->stream));
     SPK_TRY(solve(s, db, dx, s->stream, nullptr));
     if (!xd) SPK_CUDA(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream));
     SPK_CUDA(cudaStreamSynchronize(s->stream));
-    return check_device_error(s);
+    debug_check("after the partition solve", s);
+    const int rc = check_device_error(s);
+    debug_check("after the error word", s);
+    return rc;
 }
 
 int spk_check(spk_system *s) {
@@ -502,6 +530,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
     }
     if (!strcmp(name, "chain")) return s->chain_ok;
+    if (!strcmp(name, "device_check")) return chain_device_check();  // checked builds only
     if (!strcmp(name, "chains")) return s->ch_count;
     if (!strcmp(name, "chain_rows")) return s->ch_len;
     if (!strcmp(name, "chain_width")) return s->ch_width;

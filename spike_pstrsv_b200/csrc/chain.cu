@@ -52,6 +52,23 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Checked builds (-DSPK_DEVICE_CHECKS): every index of the chain kernels is
+// bounds-checked; a failed check records (code, block, index) in g_chain_check
+// (first one kept) and the access uses index 0 instead.  Off by default.
+#ifdef SPK_DEVICE_CHECKS
+__device__ unsigned long long g_chain_check;
+__device__ __noinline__ long long chk_fail(int code, long long i) {
+    atomicCAS(&g_chain_check, 0ull,
+              ((unsigned long long)code << 48) | ((unsigned long long)(blockIdx.x & 0xffffff) << 24) |
+                  (unsigned long long)(i & 0xffffff));
+    return 0;
+}
+#define CK(i, n, code) \
+    (((unsigned long long)(long long)(i) < (unsigned long long)(long long)(n)) ? (long long)(i) : chk_fail((code), (long long)(i)))
+#else
+#define CK(i, n, code) (i)
+#endif
+
 inline int nblocks(long long n, int bs = 256) { return (int)((n + bs - 1) / bs); }
 
 // ---- layout construction -----------------------------------------------------------
@@ -129,6 +146,7 @@ struct SpikeArgs {
     int reach;
     double tau;
     int *first;
+    long long nval, nptr;  // element counts (bounds of the checked build)
 };
 
 template <int C>
@@ -150,15 +168,15 @@ __global__ void __launch_bounds__(32) k_chain_spike(SpikeArgs A) {
     int sr = 0;  // slot of the current row
     for (int r = q - 1; r >= a; r--) {
         const int j = r >> 5, l = r & 31;
-        const int p0 = A.ptr[j];
-        const int w = (A.ptr[j + 1] - p0) >> 5;
+        const int p0 = A.ptr[CK(j, A.nptr, 1)];
+        const int w = (A.ptr[CK(j + 1, A.nptr, 2)] - p0) >> 5;
         double acc[C][2];
 #pragma unroll
         for (int cc = 0; cc < C; cc++) acc[cc][0] = acc[cc][1] = 0.0;
         for (int k0 = 0; k0 < w; k0 += 4) {
-            const unsigned ow = __ldg(A.off + ((p0 + (k0 >> 2) * 128) >> 2) + l);
-            const double2 va = __ldg((const double2 *)(A.val + p0 + (k0 >> 1) * 64) + l);
-            const double2 vb = __ldg((const double2 *)(A.val + p0 + ((k0 >> 1) + 1) * 64) + l);
+            const unsigned ow = __ldg(A.off + CK(((p0 + (k0 >> 2) * 128) >> 2) + l, A.nval / 4, 3));
+            const double2 va = __ldg((const double2 *)A.val + CK((p0 + (k0 >> 1) * 64) / 2 + l, A.nval / 2, 4));
+            const double2 vb = __ldg((const double2 *)A.val + CK((p0 + ((k0 >> 1) + 1) * 64) / 2 + l, A.nval / 2, 5));
             const double v4[4] = {va.x, va.y, vb.x, vb.y};
 #pragma unroll
             for (int u = 0; u < 4; u++) {
@@ -167,14 +185,14 @@ __global__ void __launch_bounds__(32) k_chain_spike(SpikeArgs A) {
                 cs -= cs >= R ? R : 0;
 #pragma unroll
                 for (int cc = 0; cc < C; cc++)
-                    acc[cc][u & 1] = fma(-v4[u], ring[cs * 32 * C + lane + 32 * cc], acc[cc][u & 1]);
+                    acc[cc][u & 1] = fma(-v4[u], ring[CK(cs * 32 * C + lane + 32 * cc, R * 32 * C, 6)], acc[cc][u & 1]);
             }
         }
         double s = 0.0;
 #pragma unroll
         for (int cc = 0; cc < C; cc++) {
             const double x = acc[cc][0] + acc[cc][1];
-            ring[sr * 32 * C + lane + 32 * cc] = x;
+            ring[CK(sr * 32 * C + lane + 32 * cc, R * 32 * C, 7)] = x;
             s += fabs(x);
         }
 #pragma unroll
@@ -200,6 +218,7 @@ struct ChainArgs {
     int mask;           // window rows - 1 (power of two >= reach + 32)
     int reach;          // widest column distance
     int sw;             // slots of the widest tile (stage size)
+    long long nval, nptr, nrd;  // element counts (bounds of the checked build)
     int *err;
     int fail_entry;     // test hook: report a failed wait and return (spk_debug_set "fail_waits")
 };
@@ -250,18 +269,17 @@ __device__ __forceinline__ ChainStage chain_stage(unsigned char *base, int s, in
 template <int W>
 __device__ __forceinline__ void stage_tile(const ChainArgs &A, const ChainStage &S, int j, int wq, int p0, int lo,
                                            int hi, int lane) {
-    const double2 *vp = (const double2 *)(A.val + p0) + lane;
-    const unsigned *op = A.off + (p0 >> 2) + lane;
+    const double2 *vp = (const double2 *)A.val;
 #pragma unroll
     for (int k = 0; k < W / 2; k++)
-        if (2 * k < wq) cpa16(&S.v[32 * k + lane], vp + 32 * k);
+        if (2 * k < wq) cpa16(&S.v[CK(32 * k + lane, 16 * A.sw, 10)], vp + CK(p0 / 2 + 32 * k + lane, A.nval / 2, 11));
 #pragma unroll
     for (int k = 0; k < W / 4; k++)
-        if (4 * k < wq) cpa4(&S.o[32 * k + lane], op + 32 * k);
+        if (4 * k < wq) cpa4(&S.o[CK(32 * k + lane, 8 * A.sw, 12)], A.off + CK((p0 >> 2) + 32 * k + lane, A.nval / 4, 13));
     const int r = 32 * j + lane;
     if (r >= lo && r < hi) {
-        cpa8(&S.rd[lane], A.rd + r);
-        cpa8(&S.b[lane], A.b + (A.rev ? A.n - 1 - r : r));
+        cpa8(&S.rd[lane], A.rd + CK(r, A.nrd, 14));
+        cpa8(&S.b[lane], A.b + CK(A.rev ? A.n - 1 - r : r, A.n, 15));
     }
 }
 
@@ -284,10 +302,10 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
             double2 v2[4];
 #pragma unroll
             for (int h = 0; h < 2; h++)
-                if (8 * g + 4 * h < W) ow[h] = S.o[32 * (2 * g + h) + lane];
+                if (8 * g + 4 * h < W) ow[h] = S.o[CK(32 * (2 * g + h) + lane, 8 * A.sw, 16)];
 #pragma unroll
             for (int h = 0; h < 4; h++)
-                if (8 * g + 2 * h < W) v2[h] = S.v[32 * (4 * g + h) + lane];
+                if (8 * g + 2 * h < W) v2[h] = S.v[CK(32 * (4 * g + h) + lane, 16 * A.sw, 17)];
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 const int k = 8 * g + u;
@@ -333,7 +351,7 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
     }
     if (act) {
         win[r & A.mask] = acc;
-        if (r >= t.st_lo && r < t.st_hi) A.x[A.rev ? A.n - 1 - r : r] = acc;
+        if (r >= t.st_lo && r < t.st_hi) A.x[CK(A.rev ? A.n - 1 - r : r, A.n, 18)] = acc;
     }
     __syncwarp();  // window rows and coefficient reads done before the next tile
 }
@@ -358,7 +376,7 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     for (int k = lane; k <= A.mask; k += 32) {
         const int r = t.hi + k;
         double v = 0.0;
-        if (PRE && r < A.n && k < A.reach) v = A.x[A.rev ? A.n - 1 - r : r];  // the coupling rows only
+        if (PRE && r < A.n && k < A.reach) v = A.x[CK(A.rev ? A.n - 1 - r : r, A.n, 19)];  // the coupling rows only
         win[r & A.mask] = v;
     }
     __syncwarp();
@@ -366,8 +384,8 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
     // slot counts of the tiles, 32 at a time: lane l holds tile (base - l)'s
     auto ptr_pair = [&](int base, int &p0, int &p1) {
         const int jj = base - lane;
-        p0 = jj >= jb ? __ldg(A.ptr + jj) : 0;
-        p1 = jj >= jb ? __ldg(A.ptr + jj + 1) : 0;
+        p0 = jj >= jb ? __ldg(A.ptr + CK(jj, A.nptr, 20)) : 0;
+        p1 = jj >= jb ? __ldg(A.ptr + CK(jj + 1, A.nptr, 21)) : 0;
     };
     int pbase = jt, pa, pb;
     ptr_pair(pbase, pa, pb);
@@ -427,6 +445,9 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.mask = s->ch_win - 1;
     A.reach = s->ch_reach;
     A.sw = s->ch_sw;
+    A.nval = (long long)s->ch_val.n;
+    A.nptr = (long long)s->ch_ptr.n;
+    A.nrd = (long long)s->rdiag.n;
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     auto go = [&](auto kern) -> int {
@@ -480,6 +501,7 @@ struct RhsArgs {
     int wr;                // window rows (>= reach + 32)
     int reach;             // widest column distance
     int sw;                // slots of the widest tile
+    long long nval, nptr, nrd;  // element counts (bounds of the checked build)
     int *err;
     int fail_entry;
 };
@@ -509,23 +531,23 @@ __device__ __forceinline__ RhsStage<T> rhs_stage(unsigned char *base, int sw) {
 template <typename T, int W>
 __device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsStage<T> &S, int j, int p0, int wq,
                                                int lo, int hi, int lane) {
-    const T *vp = A.val + p0 + 2 * lane;
-    const unsigned *op = A.off + (p0 >> 2) + lane;
 #pragma unroll
     for (int k = 0; k < W / 2; k++) {
         if (2 * k < wq) {
-            if (sizeof(T) == 8) cpa16(S.v + 64 * k + 2 * lane, vp + 64 * k);
-            else cpa8(S.v + 64 * k + 2 * lane, vp + 64 * k);
+            T *dst = S.v + CK(64 * k + 2 * lane, 32 * A.sw - 1, 30);
+            const T *src = A.val + CK(p0 + 64 * k + 2 * lane, A.nval - 1, 31);
+            if (sizeof(T) == 8) cpa16(dst, src);
+            else cpa8(dst, src);
         }
     }
 #pragma unroll
     for (int k = 0; k < W / 4; k++)
-        if (4 * k < wq) cpa4(S.o + 32 * k + lane, op + 32 * k);
+        if (4 * k < wq) cpa4(S.o + CK(32 * k + lane, 8 * A.sw, 32), A.off + CK((p0 >> 2) + 32 * k + lane, A.nval / 4, 33));
     const int r = 32 * j + lane;
     if (r >= lo && r < hi) {
-        if (sizeof(T) == 8) cpa8(S.rd + lane, A.rd + r);
-        else cpa4(S.rd + lane, A.rd + r);
-        const long long o = A.rev ? (long long)A.n - 1 - r : r;
+        if (sizeof(T) == 8) cpa8(S.rd + lane, A.rd + CK(r, A.nrd, 34));
+        else cpa4(S.rd + lane, A.rd + CK(r, A.nrd, 34));
+        const long long o = CK(A.rev ? (long long)A.n - 1 - r : r, A.n, 35);
         for (int k = 0; k < A.nk; k++) cpa8(S.b + lane * kRhsPad + k, A.B + k * A.ldb + o);
     }
 }
@@ -553,12 +575,12 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
         const bool ok = PRE && r < n && i < A.reach;
         const long long o = A.rev ? (long long)n - 1 - r : r;
         T *wr = win + (r % WR) * kRhsPad;
-        for (int k = 0; k < 32; k++) wr[k] = (ok && k < A.nk) ? (T)A.X[k * A.ldx + o] : T(0);
+        for (int k = 0; k < 32; k++) wr[k] = (ok && k < A.nk) ? (T)A.X[k * A.ldx + CK(o, n, 36)] : T(0);
     }
     const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
     auto tile_ptr = [&](int jj, int &p0, int &wq) {
-        p0 = __ldg(A.ptr + jj);
-        wq = (__ldg(A.ptr + jj + 1) - p0) >> 5;
+        p0 = __ldg(A.ptr + CK(jj, A.nptr, 37));
+        wq = (__ldg(A.ptr + CK(jj + 1, A.nptr, 38)) - p0) >> 5;
     };
     int p0n, wqn;
     tile_ptr(jt, p0n, wqn);
@@ -604,10 +626,10 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
             for (int k = 0; k < W / 2; k++) wi[lane * WIP + k] = words[k];
             // a half-filled group of eight slots: zero weights for its second half
             if (wq & 4) {
-                S.v[64 * (wq >> 1) + 2 * lane] = T(0);
-                S.v[64 * (wq >> 1) + 2 * lane + 1] = T(0);
-                S.v[64 * ((wq >> 1) + 1) + 2 * lane] = T(0);
-                S.v[64 * ((wq >> 1) + 1) + 2 * lane + 1] = T(0);
+                S.v[CK(64 * (wq >> 1) + 2 * lane, 32 * A.sw, 39)] = T(0);
+                S.v[CK(64 * (wq >> 1) + 2 * lane + 1, 32 * A.sw, 39)] = T(0);
+                S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane, 32 * A.sw, 40)] = T(0);
+                S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane + 1, 32 * A.sw, 40)] = T(0);
             }
         }
         __syncwarp();  // every lane's copies and indices are visible to the warp
@@ -626,10 +648,11 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
                     for (int h = 0; h < 4; h++) {
                         const int k = 4 * g + h;
                         if (2 * k < W) {
-                            const V2 v2 = *reinterpret_cast<const V2 *>(S.v + 64 * k + 2 * i);
+                            const V2 v2 = *reinterpret_cast<const V2 *>(S.v + CK(64 * k + 2 * i, 32 * A.sw - 1, 41));
                             const unsigned w2 = wi[i * WIP + k];
-                            p[0] = fma(v2.x, *reinterpret_cast<const T *>(wl + (w2 & 0xffffu)), p[0]);
-                            p[1] = fma(v2.y, *reinterpret_cast<const T *>(wl + (w2 >> 16)), p[1]);
+                            const int wb = WR * kRhsPad * (int)sizeof(T);
+                            p[0] = fma(v2.x, *reinterpret_cast<const T *>(wl + CK(w2 & 0xffffu, wb, 42)), p[0]);
+                            p[1] = fma(v2.y, *reinterpret_cast<const T *>(wl + CK(w2 >> 16, wb, 43)), p[1]);
                         }
                     }
                 }
@@ -647,7 +670,7 @@ __global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
                 int slot = base + lane;
                 slot -= slot >= WR ? WR : 0;
                 const T *wr = win + slot * kRhsPad;
-                for (int k = 0; k < A.nk; k++) A.X[k * A.ldx + o] = (double)wr[k];
+                for (int k = 0; k < A.nk; k++) A.X[k * A.ldx + CK(o, n, 44)] = (double)wr[k];
             }
         }
     }
@@ -680,6 +703,9 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
     A.wr = s->ch_reach + 32;
     A.reach = s->ch_reach;
     A.sw = s->ch_sw;
+    A.nval = (long long)s->ch_val.n;
+    A.nptr = (long long)s->ch_ptr.n;
+    A.nrd = (long long)(sizeof(T) == 8 ? s->rdiag.n : s->rdiagf.n);
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     const int W = s->ch_width;
@@ -722,6 +748,8 @@ int spike_firsts(spk_system *s, const std::vector<int2> &chains, std::vector<int
     A.reach = s->ch_reach;
     A.tau = s->trunc_tol;
     A.first = d_first.p;
+    A.nval = (long long)s->ch_val.n;
+    A.nptr = (long long)s->ch_ptr.n;
     const int C = s->ch_reach <= 32 ? 1 : (s->ch_reach <= 64 ? 2 : 4);
     const int smem = (int)sizeof(double) * (s->ch_reach + 1) * 32 * C;
     switch (C) {
@@ -1069,6 +1097,17 @@ int chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *
     for (i1 = i0; i1 < (int)v.size() && (phase == 1 ? v[i1].hi : v[i1].hi) <= row_hi; i1++) {}
     if (phase == 1) return launch_chain<false>(s, s->d_ctasks1.p + i0, i1 - i0, b, x, st);
     return launch_chain<true>(s, s->d_ctasks4.p + i0, i1 - i0, b, x, st);
+}
+
+// The first failed check of a checked build (0: none, or not a checked build).
+long long chain_device_check() {
+#ifdef SPK_DEVICE_CHECKS
+    unsigned long long v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_chain_check, sizeof(v)) != cudaSuccess) return -1;
+    return (long long)v;
+#else
+    return 0;
+#endif
 }
 
 // One solve through the chain path: phase 1 then phase 4 on stream st.

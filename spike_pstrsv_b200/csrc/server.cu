@@ -378,9 +378,10 @@ int spk_server_create(spk_server **out, long long hbm_budget_bytes, int nslots) 
     cudaGetDevice(&S->device);
     for (int i = 0; i < nslots; i++) {
         Slot *sl = new Slot();
-        if (cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking) != cudaSuccess) {
+        const cudaError_t ce = cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking);
+        if (ce != cudaSuccess) {
             delete sl;
-            set_error(SPK_ERR_CUDA, "cudaStreamCreate failed");
+            set_error(SPK_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(ce));
             spk_server_destroy(S);
             return SPK_ERR_CUDA;
         }

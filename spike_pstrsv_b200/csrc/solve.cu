@@ -2063,7 +2063,10 @@ inline double worst_of(double w, double v) { return (v > w || v != v) ? v : w; }
 int residual(spk_system *s, int K, const double *X, long long ldx, const double *B, long long ldb, double *R,
              long long ldr, cudaStream_t st, bool norms) {
     if (norms) SPK_CUDA(cudaMemsetAsync(s->d_norms.p, 0, sizeof(unsigned long long) * 3 * K, st));
-    if (K > 16) {
+    // the fixed-width kernels cover 1, 2, 4, 8 and 16 columns; other widths (the
+    // chain path batches any count up to 32) take the any-width kernel, which
+    // touches only columns < K
+    if (K > 16 || (K & (K - 1)) != 0) {
         SPK_CUDA(cudaFuncSetAttribute(k_rhs_residual, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(ResSmem)));
         const int ntiles = (s->n + 31) >> 5;
@@ -2079,7 +2082,10 @@ int residual(spk_system *s, int K, const double *X, long long ldx, const double 
         case 2: launch_residual<2>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 4: launch_residual<4>(s, X, ldx, B, ldb, R, ldr, st); break;
         case 8: launch_residual<8>(s, X, ldx, B, ldb, R, ldr, st); break;
-        default: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
+        case 16: launch_residual<16>(s, X, ldx, B, ldb, R, ldr, st); break;
+        default:
+            set_error(SPK_ERR_ARG, "residual of %d columns", K);
+            return SPK_ERR_ARG;
     }
     SPK_CUDA(cudaGetLastError());
     if (norms) {

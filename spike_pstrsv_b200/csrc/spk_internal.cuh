@@ -196,6 +196,7 @@ int solve_prepare(spk_system *s);
 int chain_prepare(spk_system *s);
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);
+long long chain_device_check();
 int chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *b, double *x, cudaStream_t st);
 int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long ldb, double *X, long long ldx,
                     cudaStream_t st);
