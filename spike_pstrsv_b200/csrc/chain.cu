@@ -41,7 +41,10 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <set>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "spk_internal.cuh"
@@ -70,6 +73,27 @@ __device__ __noinline__ long long chk_fail(int code, long long i) {
 #endif
 
 inline int nblocks(long long n, int bs = 256) { return (int)((n + bs - 1) / bs); }
+
+// The dynamic shared memory a kernel may take, raised once per kernel and device
+// to the device's opt-in maximum.  Launches of the same kernel for systems of
+// different sizes come from several host threads (the serving loop's workers);
+// setting the attribute to each launch's own size would race with the launches
+// of other threads.
+template <typename K>
+int allow_smem(K kern) {
+    static std::mutex mu;
+    static std::set<std::pair<int, const void *>> done;
+    int dev = 0;
+    SPK_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(dev, (const void *)kern);
+    if (done.count(key)) return SPK_OK;
+    int mx = 0;
+    SPK_CUDA(cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    done.insert(key);
+    return SPK_OK;
+}
 
 // ---- layout construction -----------------------------------------------------------
 
@@ -452,7 +476,7 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.fail_entry = s->dbg_fail_waits > 0;
     auto go = [&](auto kern) -> int {
         const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
-        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_TRY(allow_smem(kern));
         kern<<<ntasks, 32, smem, st>>>(A);
         SPK_CUDA(cudaGetLastError());
         return SPK_OK;
@@ -711,7 +735,7 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
     const int W = s->ch_width;
     const size_t smem = rhs_smem_bytes(s, sizeof(T));
     auto go = [&](auto kern) -> int {
-        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_TRY(allow_smem(kern));
         kern<<<ntasks, 32, smem, st>>>(A);
         SPK_CUDA(cudaGetLastError());
         return SPK_OK;
@@ -754,15 +778,15 @@ int spike_firsts(spk_system *s, const std::vector<int2> &chains, std::vector<int
     const int smem = (int)sizeof(double) * (s->ch_reach + 1) * 32 * C;
     switch (C) {
         case 1:
-            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            SPK_TRY(allow_smem(k_chain_spike<1>));
             k_chain_spike<1><<<A.nchains, 32, smem, s->stream>>>(A);
             break;
         case 2:
-            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            SPK_TRY(allow_smem(k_chain_spike<2>));
             k_chain_spike<2><<<A.nchains, 32, smem, s->stream>>>(A);
             break;
         default:
-            SPK_CUDA(cudaFuncSetAttribute(k_chain_spike<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            SPK_TRY(allow_smem(k_chain_spike<4>));
             k_chain_spike<4><<<A.nchains, 32, smem, s->stream>>>(A);
             break;
     }
@@ -954,7 +978,7 @@ int build_plan(spk_system *s, long long len, int reach, bool batch) {
 int chain_occupancy(spk_system *s, int *occ) {
     const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
     auto q = [&](auto kern) -> int {
-        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_TRY(allow_smem(kern));
         SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
         return SPK_OK;
     };
@@ -972,7 +996,7 @@ int chain_rhs_occupancy(spk_system *s, int *occ) {
     const int W = s->ch_width;
     const size_t smem = rhs_smem_bytes(s, sizeof(double));
     auto q = [&](auto kern) -> int {
-        SPK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        SPK_TRY(allow_smem(kern));
         SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
         return SPK_OK;
     };
