@@ -538,8 +538,8 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "chain_rows_phase1")) return s->ch_rows1;
     if (!strcmp(name, "chain_rows_phase4")) return s->ch_rows4;
     if (!strcmp(name, "chain_tasks_phase4")) return s->nctasks4;
-    if (!strcmp(name, "chain_batch_rows")) return s->chb_len;
-    if (!strcmp(name, "chain_batch_tasks_phase4")) return s->nbtasks1 ? s->nbtasks4 : s->nctasks4;
+    if (!strcmp(name, "chain_batch_rows")) return s->cp_batch.len ? s->cp_batch.len : s->ch_len;
+    if (!strcmp(name, "chain_host_rows")) return s->cp_host.len ? s->cp_host.len : s->ch_len;
     if (!strcmp(name, "chain_bytes")) return (long long)(s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes());
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;
     if (!strcmp(name, "kept_reduced_rows")) return s->nkept;
@@ -553,7 +553,8 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
         b += s->ell_valf.bytes() + s->rdiagf.bytes() + s->diag.bytes() + s->rbuf.bytes() + s->dbuf.bytes() + s->work.bytes();
         b += s->stage_b.bytes() + s->stage_x.bytes();
-        b += s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes() + s->d_ctasks1.bytes() + s->d_ctasks4.bytes();
+        b += s->ch_val.bytes() + s->ch_valf.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes() + s->d_ctasks1.bytes() +
+             s->d_ctasks4.bytes();
         return b;
     }
     return -1;

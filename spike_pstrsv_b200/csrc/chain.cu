@@ -266,7 +266,8 @@ __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_gro
 template <int N>
 __device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-constexpr int kChainStages = 3;  // tiles in shared memory: the one solved + two in flight
+// tiles staged in shared memory per task: the one solved + NS - 1 in flight (NS is
+// a template parameter of the solve kernel, 2 or 3: s->ch_stages)
 
 // One staged tile (sw = the widest tile's slots, a multiple of 4).  Lane l
 // copies (and later reads) only its own row: value pairs v[(k/2)*32 + l],
@@ -382,8 +383,9 @@ __device__ __forceinline__ void solve_tile(const ChainArgs &A, const ChainStage 
 
 // PRE: phase 4 (the window starts with x of rows [hi, hi + window)); else
 // phase 1 (it starts at zero: zero coupling beyond the chain).
-template <bool PRE, int W>
+template <bool PRE, int W, int NS>
 __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
+    constexpr int kChainStages = NS;
     extern __shared__ __align__(16) unsigned char smc[];
     ChainStage stg[kChainStages];
 #pragma unroll
@@ -437,7 +439,7 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
         for (int s = 0; s < kChainStages; s++) {
             const int j = j0 - s;
             if (j >= jb) {
-                const int sl = (s + kChainStages - 1) % kChainStages;  // stage of tile j - 2
+                const int sl = (s + kChainStages - 1) % kChainStages;  // stage of tile j - (NS - 1)
                 const int jl = j - (kChainStages - 1);
                 if (jl >= jb) {
                     int p0;
@@ -451,6 +453,10 @@ __global__ void __launch_bounds__(32) k_chain_solve(ChainArgs A) {
         }
     }
     cpa_wait<0>();
+}
+
+size_t chain_smem_bytes(const spk_system *s) {
+    return (size_t)s->ch_stages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
 }
 
 template <bool PRE>
@@ -475,18 +481,27 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
     auto go = [&](auto kern) -> int {
-        const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
         SPK_TRY(allow_smem(kern));
-        kern<<<ntasks, 32, smem, st>>>(A);
+        kern<<<ntasks, 32, chain_smem_bytes(s), st>>>(A);
         SPK_CUDA(cudaGetLastError());
         return SPK_OK;
     };
-    switch (s->ch_width) {
-        case 4: SPK_TRY(go(k_chain_solve<PRE, 4>)); break;
-        case 8: SPK_TRY(go(k_chain_solve<PRE, 8>)); break;
-        case 16: SPK_TRY(go(k_chain_solve<PRE, 16>)); break;
-        case 32: SPK_TRY(go(k_chain_solve<PRE, 32>)); break;
-        default: SPK_TRY(go(k_chain_solve<PRE, 64>)); break;
+    if (s->ch_stages == 2) {
+        switch (s->ch_width) {
+            case 4: SPK_TRY(go(k_chain_solve<PRE, 4, 2>)); break;
+            case 8: SPK_TRY(go(k_chain_solve<PRE, 8, 2>)); break;
+            case 16: SPK_TRY(go(k_chain_solve<PRE, 16, 2>)); break;
+            case 32: SPK_TRY(go(k_chain_solve<PRE, 32, 2>)); break;
+            default: SPK_TRY(go(k_chain_solve<PRE, 64, 2>)); break;
+        }
+    } else {
+        switch (s->ch_width) {
+            case 4: SPK_TRY(go(k_chain_solve<PRE, 4, 3>)); break;
+            case 8: SPK_TRY(go(k_chain_solve<PRE, 8, 3>)); break;
+            case 16: SPK_TRY(go(k_chain_solve<PRE, 16, 3>)); break;
+            case 32: SPK_TRY(go(k_chain_solve<PRE, 32, 3>)); break;
+            default: SPK_TRY(go(k_chain_solve<PRE, 64, 3>)); break;
+        }
     }
     s->launches++;
     return SPK_OK;
@@ -824,10 +839,9 @@ void chain_release(spk_system *s) {
     s->ch_ptr.release();
     s->d_ctasks1.release();
     s->d_ctasks4.release();
-    s->d_btasks1.release();
-    s->d_btasks4.release();
-    s->nbtasks1 = s->nbtasks4 = 0;
-    s->chb_len = 0;
+    s->cp_batch.release();
+    s->cp_host.release();
+    s->host_plan_tried = 0;
     s->h_ctasks1.clear();
     s->h_ctasks4.clear();
     s->nctasks1 = s->nctasks4 = 0;
@@ -840,7 +854,7 @@ void chain_release(spk_system *s) {
 
 int chain_occupancy(spk_system *s, int *occ);
 int chain_rhs_occupancy(spk_system *s, int *occ);
-int build_plan(spk_system *s, long long len, int reach, bool batch);
+int build_plan(spk_system *s, long long len, int reach, ChainPlan *extra);
 
 // Build the chain layout, the chains' spikes and the two task lists; leaves
 // chain_ok = 0 (the partition-based solve) when truncation is off, the layout
@@ -877,6 +891,8 @@ int chain_prepare(spk_system *s) {
     ptr[ntiles] = (int)tot;
     s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : (wmax <= 32 ? 32 : 64)));
     s->ch_sw = (wmax + 7) & ~7;  // stages hold whole groups of eight slots
+    s->ch_stages = 3;
+    if (const char *e = getenv("SPK_CHAIN_STAGES")) s->ch_stages = atoi(e) == 2 ? 2 : 3;
     s->ch_reach = reach;
     int win = 64;
     while (win < reach + 32) win <<= 1;
@@ -898,7 +914,7 @@ int chain_prepare(spk_system *s) {
     long long len = 32ll * ((n / (sms * (long long)std::min(std::max(occ, 1), 7)) + 31) / 32);
     len = std::max<long long>(len, 1024);
     if (const char *e = getenv("SPK_CHAIN_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
-    SPK_TRY(build_plan(s, len, reach, false));
+    SPK_TRY(build_plan(s, len, reach, nullptr));
     if (!s->chain_ok) return SPK_OK;
     // the batched kernel keeps fewer tasks resident (a wider window): its own
     // chains, as many as it keeps resident
@@ -907,21 +923,21 @@ int chain_prepare(spk_system *s) {
     long long lenb = 32ll * ((n / (sms * (long long)std::max(occb, 1)) + 31) / 32);
     lenb = std::max<long long>(lenb, s->ch_len);
     if (const char *e = getenv("SPK_CHAIN_BATCH_ROWS")) lenb = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
-    SPK_TRY(build_plan(s, lenb, reach, true));
+    if (lenb > s->ch_len) SPK_TRY(build_plan(s, lenb, reach, &s->cp_batch));
     return SPK_OK;
 }
 
 // Chains of `len` rows (doubled up to three times until every chain keeps its
 // first `reach` rows, never fewer than 8 chains): their spikes, the two task
 // lists (row order: the pipelined and sharded solves launch them by row range).
-// batch = false: the plain solve's plan (sets chain_ok, or releases everything
-// when no length is valid); true: the batched kernel's plan (falls back to the
-// plain plan's tasks when no length is valid).
-int build_plan(spk_system *s, long long len, int reach, bool batch) {
+// extra == nullptr: the plain solve's plan (sets chain_ok, or releases everything
+// when no length is valid); else a second plan (left unbuilt, so that the plain
+// plan's tasks are used, when no length short of the plain one is valid).
+int build_plan(spk_system *s, long long len, int reach, ChainPlan *extra) {
     const int n = s->n;
     const long long max_len = std::min<long long>(8 * len, std::max<long long>(len, 32ll * ((n / 8 + 31) / 32)));
     for (; len <= max_len; len *= 2) {
-        if (batch && len == s->ch_len) break;  // the same chains as the plain solve
+        if (extra && len == s->ch_len) break;  // the same chains as the plain solve
         std::vector<int2> chains;
         for (long long a = 0; a < n; a += len)
             chains.push_back(make_int2((int)a, (int)std::min<long long>(a + len, n)));
@@ -942,12 +958,12 @@ int build_plan(spk_system *s, long long len, int reach, bool batch) {
                 rows4 += q - f;
             }
         }
-        if (batch) {
-            SPK_TRY(upload_vec(s->d_btasks1, t1));
-            SPK_TRY(upload_vec(s->d_btasks4, t4));
-            s->nbtasks1 = (int)t1.size();
-            s->nbtasks4 = (int)t4.size();
-            s->chb_len = (int)len;
+        if (extra) {
+            SPK_TRY(upload_vec(extra->d1, t1));
+            SPK_TRY(upload_vec(extra->d4, t4));
+            extra->h1 = t1;
+            extra->h4 = t4;
+            extra->len = (int)len;
             return SPK_OK;
         }
         s->h_ctasks1 = t1;
@@ -963,11 +979,8 @@ int build_plan(spk_system *s, long long len, int reach, bool batch) {
         s->chain_ok = 1;
         return SPK_OK;
     }
-    if (batch) {
-        s->d_btasks1.release();
-        s->d_btasks4.release();
-        s->nbtasks1 = s->nbtasks4 = 0;
-        s->chb_len = s->ch_len;  // the batched kernel takes the plain solve's tasks
+    if (extra) {
+        extra->release();  // the plain solve's tasks are used
         return SPK_OK;
     }
     chain_release(s);
@@ -976,18 +989,19 @@ int build_plan(spk_system *s, long long len, int reach, bool batch) {
 
 // Resident blocks per SM of the phase-1 solve kernel (its shared memory bounds it).
 int chain_occupancy(spk_system *s, int *occ) {
-    const size_t smem = kChainStages * chain_stage_bytes(s->ch_sw) + sizeof(double) * (32 * 32 + 16 + s->ch_win);
+    const size_t smem = chain_smem_bytes(s);
     auto q = [&](auto kern) -> int {
         SPK_TRY(allow_smem(kern));
         SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
         return SPK_OK;
     };
+    const bool two = s->ch_stages == 2;
     switch (s->ch_width) {
-        case 4: return q(k_chain_solve<false, 4>);
-        case 8: return q(k_chain_solve<false, 8>);
-        case 16: return q(k_chain_solve<false, 16>);
-        case 32: return q(k_chain_solve<false, 32>);
-        default: return q(k_chain_solve<false, 64>);
+        case 4: return two ? q(k_chain_solve<false, 4, 2>) : q(k_chain_solve<false, 4, 3>);
+        case 8: return two ? q(k_chain_solve<false, 8, 2>) : q(k_chain_solve<false, 8, 3>);
+        case 16: return two ? q(k_chain_solve<false, 16, 2>) : q(k_chain_solve<false, 16, 3>);
+        case 32: return two ? q(k_chain_solve<false, 32, 2>) : q(k_chain_solve<false, 32, 3>);
+        default: return two ? q(k_chain_solve<false, 64, 2>) : q(k_chain_solve<false, 64, 3>);
     }
 }
 
@@ -1019,7 +1033,20 @@ int chain_rhs_occupancy(spk_system *s, int *occ) {
 // cudaMemcpyAsync per chunk and direction; overlap needs page-locked b and x
 // (pageable memory gives the same result with the copies serialised).
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx) {
-    const int n = s->n, nch = s->nctasks1;
+    // After the last copy lands, one chain still has to be solved before its rows
+    // can leave: the pipeline takes chains of at most 2,048 rows (built once,
+    // on the first host-array solve) to shorten that tail.
+    if (!s->host_plan_tried) {
+        s->host_plan_tried = 1;
+        long long len = 2048;
+        if (const char *e = getenv("SPK_PIPELINE_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
+        if (len < s->ch_len) SPK_TRY(build_plan(s, len, s->ch_reach, &s->cp_host));
+    }
+    const ChainPlan &hp = s->cp_host;
+    const bool own = hp.len > 0;
+    const std::vector<ChainTask> &T1 = own ? hp.h1 : s->h_ctasks1, &T4 = own ? hp.h4 : s->h_ctasks4;
+    const ChainTask *D1 = own ? hp.d1.p : s->d_ctasks1.p, *D4 = own ? hp.d4.p : s->d_ctasks4.p;
+    const int n = s->n, nch = (int)T1.size(), n4 = (int)T4.size();
     int K = 16;
     if (const char *e = getenv("SPK_PIPELINE_CHUNKS")) K = std::max(1, atoi(e));
     K = std::min(K, std::max(nch, 1));
@@ -1046,13 +1073,13 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
         int t = 0;
         for (int k = 0; k < K; k++) {
             t0[k] = t;
-            const int qend = s->h_ctasks1[c0[k + 1] - 1].hi;
-            while (t < s->nctasks4 && s->h_ctasks4[t].hi <= qend) t++;
+            const int qend = T1[c0[k + 1] - 1].hi;
+            while (t < n4 && T4[t].hi <= qend) t++;
         }
-        t0[K] = s->nctasks4;
+        t0[K] = n4;
     }
     auto lo_rows = [&](int k, int &lo, int &cnt) {
-        const int A = s->h_ctasks1[c0[k]].lo, Q = s->h_ctasks1[c0[k + 1] - 1].hi;
+        const int A = T1[c0[k]].lo, Q = T1[c0[k + 1] - 1].hi;
         lo = rev ? n - Q : A;
         cnt = Q - A;
     };
@@ -1069,13 +1096,13 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
     for (int k = 0; k < K; k++) {
         cudaStream_t q = s->pipe_st[k];
         SPK_CUDA(cudaStreamWaitEvent(q, ev_in[k], 0));
-        SPK_TRY(launch_chain<false>(s, s->d_ctasks1.p + c0[k], c0[k + 1] - c0[k], db, dx, q));
+        SPK_TRY(launch_chain<false>(s, D1 + c0[k], c0[k + 1] - c0[k], db, dx, q));
         SPK_CUDA(cudaEventRecord(ev_p1[k], q));
     }
     for (int k = 0; k < K; k++) {
         cudaStream_t q = s->pipe_st[k];
         if (k + 1 < K) SPK_CUDA(cudaStreamWaitEvent(q, ev_p1[k + 1], 0));
-        SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p + t0[k], t0[k + 1] - t0[k], db, dx, q));
+        SPK_TRY(launch_chain<true>(s, D4 + t0[k], t0[k + 1] - t0[k], db, dx, q));
         SPK_CUDA(cudaEventRecord(ev_done[k], q));
         int lo, cnt;
         lo_rows(k, lo, cnt);
@@ -1098,9 +1125,10 @@ int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long 
         set_error(SPK_ERR_ARG, "chain batch of %d columns (1..32)", nk);
         return SPK_ERR_ARG;
     }
-    const bool own = s->nbtasks1 > 0;  // the batched kernel's own chains
-    const ChainTask *t1 = own ? s->d_btasks1.p : s->d_ctasks1.p, *t4 = own ? s->d_btasks4.p : s->d_ctasks4.p;
-    const int n1 = own ? s->nbtasks1 : s->nctasks1, n4 = own ? s->nbtasks4 : s->nctasks4;
+    const ChainPlan &bp = s->cp_batch;
+    const bool own = bp.len > 0;  // the batched kernel's own chains
+    const ChainTask *t1 = own ? bp.d1.p : s->d_ctasks1.p, *t4 = own ? bp.d4.p : s->d_ctasks4.p;
+    const int n1 = own ? (int)bp.h1.size() : s->nctasks1, n4 = own ? (int)bp.h4.size() : s->nctasks4;
     if (fp32) {
         SPK_TRY(chain_fp32(s));
         SPK_TRY((launch_chain_rhs<float, false>(s, t1, n1, nk, B, ldb, X, ldx, st)));

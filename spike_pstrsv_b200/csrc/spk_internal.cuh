@@ -106,6 +106,22 @@ struct ChainTask {
     int st_lo, st_hi;
 };
 
+// A second chain decomposition of the same rows (the batched kernel's longer
+// chains, the host-array pipeline's shorter ones): task lists on the device and
+// the host (row order).
+struct ChainPlan {
+    DBuf<ChainTask> d1, d4;
+    std::vector<ChainTask> h1, h4;
+    int len = 0;  // 0: not built (the plain solve's chains are used)
+    void release() {
+        d1.release();
+        d4.release();
+        h1.clear();
+        h4.clear();
+        len = 0;
+    }
+};
+
 // Truncation threshold on absolute spike-row sums (2^-60, below FP64 resolution
 // relative to ||x||_inf); negative = exact mode (nothing dropped).
 constexpr double kDefaultTruncTol = 8.673617379884035e-19;
@@ -153,14 +169,15 @@ struct spk_system {
     char *ext_ws = nullptr;  // caller-lent device workspace for the batched solves (spk_set_workspace)
     size_t ext_ws_bytes = 0;  // largest column distance from a tile's first row (-1: not computed)
     // chain solver (default one-right-hand-side solve; chain.cu)
-    int chain_ok = 0, ch_width = 0, ch_sw = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0;
+    int chain_ok = 0, ch_width = 0, ch_sw = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0, ch_stages = 3;
     spk::DBuf<double> ch_val;          // row-scaled off-diagonals, sliced ELL
     spk::DBuf<float> ch_valf;          // their FP32 copy (batched FP32 solves, made on first use)
     spk::DBuf<unsigned char> ch_off;   // column offsets c - r (8 bits)
     spk::DBuf<int> ch_ptr;             // first slot of each 32-row tile
     spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;
-    spk::DBuf<spk::ChainTask> d_btasks1, d_btasks4;  // the batched kernel's own chains (longer)
-    int nbtasks1 = 0, nbtasks4 = 0, chb_len = 0;
+    spk::ChainPlan cp_batch;  // the batched kernel's own chains (longer; built at preprocessing)
+    spk::ChainPlan cp_host;   // the host-array pipeline's chains (shorter; built on first use)
+    int host_plan_tried = 0;
     int nctasks1 = 0, nctasks4 = 0;
     long long ch_rows1 = 0, ch_rows4 = 0;
     std::vector<spk::ChainTask> h_ctasks1, h_ctasks4;
