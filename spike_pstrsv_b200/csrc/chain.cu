@@ -27,7 +27,7 @@
 // a(r,c)/a(r,r) (so x_r = b_r/a(r,r) - sum v'(r,c) x_c) with 8-bit column
 // offsets c - r, per tile slot-pair-major (values: one 16-byte copy per lane per
 // two slots; offsets: one 4-byte copy per lane per four slots).  Each tile is
-// staged into shared memory by cp.async two tiles ahead; every lane copies and
+// staged into shared memory by cp.async one tile ahead; every lane copies and
 // reads only its own row, so a stage needs no barrier.  Shared memory also holds
 // the solved-row window (gathers of far columns) and a per-lane column of
 // in-tile coefficients: coef[i][lane] = v'(row0+lane, row0+i) is written and
@@ -891,8 +891,10 @@ int chain_prepare(spk_system *s) {
     ptr[ntiles] = (int)tot;
     s->ch_width = wmax <= 4 ? 4 : (wmax <= 8 ? 8 : (wmax <= 16 ? 16 : (wmax <= 32 ? 32 : 64)));
     s->ch_sw = (wmax + 7) & ~7;  // stages hold whole groups of eight slots
-    s->ch_stages = 3;
-    if (const char *e = getenv("SPK_CHAIN_STAGES")) s->ch_stages = atoi(e) == 2 ? 2 : 3;
+    // two stages (one tile in flight) measured as fast as three on the banded
+    // workload and leave room for more resident tasks when tiles are wide
+    s->ch_stages = 2;
+    if (const char *e = getenv("SPK_CHAIN_STAGES")) s->ch_stages = atoi(e) == 3 ? 3 : 2;
     s->ch_reach = reach;
     int win = 64;
     while (win < reach + 32) win <<= 1;

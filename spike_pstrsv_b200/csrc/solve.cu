@@ -2283,8 +2283,11 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     SPK_CUDA(cudaGetDevice(&dev0));
     SPK_CUDA(cudaDeviceGetAttribute(&sms0, cudaDevAttrMultiProcessorCount, dev0));
     const bool part_wide = std::min(s->redNec ? s->ntasks1 : s->ntasks2, s->ntasks2) >= 2 * sms0;
+    // FP64: the chain kernel (faster than the partition kernels at every partition
+    // count measured); FP32 + refinement: the chain kernel when the partitions give
+    // too few tasks to fill the GPU
     const char *cb = getenv("SPK_CHAIN_BATCH");  // 1: always the chain kernels, 0: never
-    const bool use_chain = s->chain_ok && (cb ? cb[0] == '1' : !part_wide);
+    const bool use_chain = s->chain_ok && (cb ? cb[0] == '1' : (mode == 0 || !part_wide));
     if (use_chain) {
         // the chain tasks fill the GPU whatever the partition count: every group
         // of up to 32 columns is one right-hand-side-parallel chain solve (used
