@@ -553,7 +553,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         b += s->rdiag.bytes() + s->ell_val.bytes() + s->ell_col.bytes() + s->ell_ptr.bytes();
         b += s->ell_valf.bytes() + s->rdiagf.bytes() + s->diag.bytes() + s->rbuf.bytes() + s->dbuf.bytes() + s->work.bytes();
         b += s->stage_b.bytes() + s->stage_x.bytes();
-        b += s->ch_val.bytes() + s->ch_valf.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes() + s->d_ctasks1.bytes() +
+        b += s->ch_val.bytes() + s->ch_valb.bytes() + s->ch_valbf.bytes() + s->ch_near.bytes() + s->ch_nearf.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes() + s->d_ctasks1.bytes() +
              s->d_ctasks4.bytes();
         return b;
     }

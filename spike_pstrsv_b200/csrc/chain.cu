@@ -507,26 +507,37 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
     return SPK_OK;
 }
 
-// ---- many right-hand sides: lane = right-hand side ---------------------------------------
+// ---- many right-hand sides --------------------------------------------------------------
 //
-// The same chains and tasks, up to 32 right-hand sides per warp: lane k owns
-// right-hand side k and walks the task's rows bottom-up, so every window access
-// of a lane is to its own column and the row-to-row dependency needs no
-// barrier.  The window [WR][33] (T, WR = reach + 32 rows, row r at r mod WR)
-// holds x of the solved rows.  A tile (32 rows) is staged by cp.async one tile
-// ahead, each lane copying its own row: the slot values (T) and offsets, 1/diag
-// and the row's right-hand sides b[row][0..nk) (FP64).  When a tile has landed,
-// each lane turns its row's offsets into window element indices (row of the
-// column mod WR, times 33), so that a slot in the row loop is one broadcast
-// index, one window load and one fused multiply-add.  Solved rows leave the
-// window through a transpose (lane = row, coalesced along rows).
-
-constexpr int kRhsPad = 33;
+// The same chains and tasks, up to 32 right-hand sides per pass.  A block of
+// one or two warps walks one task bottom-up and shares its staged tiles; warp
+// w owns right-hand sides [RPW w, RPW (w+1)) of the pass (RPW = 16 in FP64, 32
+// in FP32) and a window of its own: [WR][9 vectors of 16 bytes] (row r at r mod
+// WR, WR = reach + 32), eight vectors of right-hand sides and one of padding.
+// Lane (q, kv) = (lane / 8, lane % 8) solves the row at place q of each group of
+// four rows for the 16-byte vector kv of right-hand sides (2 FP64 or 4 FP32),
+// so a quarter warp reads one window row as 128 contiguous bytes (no bank
+// conflicts) and every load, address and slot weight serves a whole vector.
+//
+// A row's coefficients at offsets inside its own group (at most three, fixed
+// by the row's place, row mod 4) are kept apart at preprocessing: the slot
+// values the kernel reads have them zeroed, and near[row][0..3] holds them in
+// the order the in-group chain applies them.  So the slot sums of the four rows
+// read only rows of earlier groups and run side by side; the chain then hands
+// each place's values to the lanes below it by shuffles (three steps).
+//
+// A tile (32 rows) is staged by cp.async one tile ahead: slot values and
+// offsets, 1/diag and the near coefficients.  When it has landed, each row's
+// offsets become window byte offsets (row of the column mod WR, times 144).
+// Right-hand sides are read straight into registers a group ahead of use;
+// solved rows go to X from the row loop (one warp) or through a transpose of
+// the tile (lane = row, two warps).
 
 template <typename T>
 struct RhsArgs {
     const ChainTask *tasks;
-    const T *val;          // row-scaled values in T, chain layout
+    const T *val;          // row-scaled values in T, chain layout, in-group coefficients zeroed
+    const T *near;         // [rows][4] in-group coefficients in order of use
     const unsigned *off;
     const int *ptr;
     const T *rd;           // 1 / diagonal in T
@@ -537,24 +548,52 @@ struct RhsArgs {
     long long ldx;
     int rev;
     int nk;                // right-hand sides in this pass (<= 32)
-    int wr;                // window rows (>= reach + 32)
+    int wr;                // window rows (reach + 32)
     int reach;             // widest column distance
     int sw;                // slots of the widest tile
-    long long nval, nptr, nrd;  // element counts (bounds of the checked build)
+    long long nval, nptr, nrd, nnear;  // element counts (bounds of the checked build)
     int *err;
     int fail_entry;
 };
+
+// Shared-memory vector loads and stores by 32-bit address (volatile with a
+// memory clobber, so that the compiler keeps them in order with the other
+// accesses of the window; the hardware schedule is left to the assembler).
+__device__ __forceinline__ double2 lds_v(unsigned a, double2) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ float4 lds_v(unsigned a, float4) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void sts_v(unsigned a, double2 v) {
+    asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.x), "d"(v.y) : "memory");
+}
+__device__ __forceinline__ void sts_v(unsigned a, float4 v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+
+constexpr int kRowBytes = 144;  // a window row: 8 vectors of right-hand sides + 1 of padding
+
+// Words of window offsets per row, one per slot: W rounded up to whole 16-byte
+// units, an odd number of them (conflict-free 16-byte stores per quarter warp).
+__host__ __device__ constexpr int rhs_wi_stride(int W) {
+    return 4 * ((W / 4) | 1);
+}
 
 template <typename T>
 struct RhsStage {
     T *v;         // [32 sw] as copied: pair (k/2)*32 + l holds slots k, k+1 of row l
     unsigned *o;  // [8 sw]  offset words (k/4)*32 + l
-    double *b;    // [32][33] right-hand sides, row-major
     T *rd;        // [32]
+    T *nr;        // [32][4] near coefficients
 };
 
 __host__ __device__ __forceinline__ int rhs_stage_bytes(int sw, int tsize) {
-    return 32 * sw * tsize + 32 * sw + 32 * kRhsPad * 8 + 32 * 8;
+    return 32 * sw * tsize + 32 * sw + 32 * 8 + 128 * tsize;
 }
 
 template <typename T>
@@ -562,17 +601,19 @@ __device__ __forceinline__ RhsStage<T> rhs_stage(unsigned char *base, int sw) {
     RhsStage<T> S;
     S.v = (T *)base;
     S.o = (unsigned *)(base + 32 * sw * sizeof(T));
-    S.b = (double *)(base + 32 * sw * sizeof(T) + 32 * sw);
-    S.rd = (T *)(S.b + 32 * kRhsPad);
+    S.rd = (T *)(base + 32 * sw * sizeof(T) + 32 * sw);
+    S.nr = (T *)(base + 32 * sw * sizeof(T) + 32 * sw + 32 * 8);
     return S;
 }
 
+// cp.async of tile j: warp w copies the slot pairs k with k % nw == w (lane =
+// row); warp 0 also 1/diag and the near coefficients of the task's rows.
 template <typename T, int W>
 __device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsStage<T> &S, int j, int p0, int wq,
-                                               int lo, int hi, int lane) {
+                                               int lo, int hi, int lane, int w, int nw) {
 #pragma unroll
     for (int k = 0; k < W / 2; k++) {
-        if (2 * k < wq) {
+        if (k % nw == w && 2 * k < wq) {
             T *dst = S.v + CK(64 * k + 2 * lane, 32 * A.sw - 1, 30);
             const T *src = A.val + CK(p0 + 64 * k + 2 * lane, A.nval - 1, 31);
             if (sizeof(T) == 8) cpa16(dst, src);
@@ -581,157 +622,281 @@ __device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsSta
     }
 #pragma unroll
     for (int k = 0; k < W / 4; k++)
-        if (4 * k < wq) cpa4(S.o + CK(32 * k + lane, 8 * A.sw, 32), A.off + CK((p0 >> 2) + 32 * k + lane, A.nval / 4, 33));
+        if (k % nw == w && 4 * k < wq)
+            cpa4(S.o + CK(32 * k + lane, 8 * A.sw, 32), A.off + CK((p0 >> 2) + 32 * k + lane, A.nval / 4, 33));
     const int r = 32 * j + lane;
-    if (r >= lo && r < hi) {
+    if (w == 0 && r >= lo && r < hi) {
         if (sizeof(T) == 8) cpa8(S.rd + lane, A.rd + CK(r, A.nrd, 34));
         else cpa4(S.rd + lane, A.rd + CK(r, A.nrd, 34));
-        const long long o = CK(A.rev ? (long long)A.n - 1 - r : r, A.n, 35);
-        for (int k = 0; k < A.nk; k++) cpa8(S.b + lane * kRhsPad + k, A.B + k * A.ldb + o);
+        for (int c = 0; c < 4 * (int)sizeof(T); c += 16)
+            cpa16((char *)(S.nr + 4 * lane) + c, (const char *)(A.near + CK(4ll * r, A.nnear - 3, 46)) + c);
     }
 }
 
+// The batched kernel's slot values and near coefficients (one thread per row
+// of the chain layout, padding rows of the last tile included): a row at place
+// p = 3 - (row mod 4) of its group of four has its coefficients at offsets
+// 1..p moved out of the slots into near[row] = {coef at offset p, p-1, p-2, 0}
+// (zero where the offset would be below 1): step d of the in-group chain applies
+// entry d, the coefficient of the row at place d.
+__global__ void k_chain_near(long long rows, const int *ptr, const double *val, const unsigned *off, double *valb,
+                             double *near) {
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const long long j = r >> 5;
+    const int l = (int)(r & 31);
+    const int p0 = ptr[j], wq = (ptr[j + 1] - p0) >> 5;
+    const int p = 3 - (l & 3);
+    double n1 = 0.0, n2 = 0.0, n3 = 0.0;
+    for (int k = 0; k < wq; k++) {
+        const long long e = (long long)p0 + 64 * (k >> 1) + 2 * l + (k & 1);
+        const unsigned ow = off[(p0 >> 2) + 32 * (k >> 2) + l];
+        const int o = (int)((ow >> (8 * (k & 3))) & 0xff);
+        double v = val[e];
+        if (o >= 1 && o <= p) {
+            n1 += o == 1 ? v : 0.0;
+            n2 += o == 2 ? v : 0.0;
+            n3 += o == 3 ? v : 0.0;
+            v = 0.0;
+        }
+        valb[e] = v;
+    }
+    double *nr = near + 4 * r;
+    nr[0] = p == 1 ? n1 : (p == 2 ? n2 : (p == 3 ? n3 : 0.0));
+    nr[1] = p == 2 ? n1 : (p == 3 ? n2 : 0.0);
+    nr[2] = p == 3 ? n1 : 0.0;
+    nr[3] = 0.0;
+}
+
 template <typename T, int W, bool PRE>
-__global__ void __launch_bounds__(32) k_chain_rhs(RhsArgs<T> A) {
+__global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
     using V2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
-    constexpr int WIP = W / 2 + 1;  // packed window indices per row (stride, words)
+    using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;  // 16 bytes
+    constexpr int V = 16 / (int)sizeof(T);  // right-hand sides per lane
+    constexpr int RPW = 8 * V;              // right-hand sides per warp
+    constexpr int WS = rhs_wi_stride(W);    // window offsets per row (words, one per slot)
     extern __shared__ __align__(16) unsigned char smr[];
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
+    const int q = lane >> 3, kv = lane & 7;  // place in the group of four, vector of right-hand sides
     if (A.fail_entry) {
-        if (lane == 0) atomicExch(A.err, 1);
+        if (tid == 0) atomicExch(A.err, 1);
         return;
     }
     const int WR = A.wr;
     const int sb = rhs_stage_bytes(A.sw, sizeof(T));
-    unsigned *wi = (unsigned *)(smr + 2 * sb);                  // [32][WIP] two 16-bit indices per word
-    T *win = (T *)(smr + 2 * sb + ((32 * WIP * 4 + 15) & ~15));  // [WR][33]
+    unsigned *wi = (unsigned *)(smr + 2 * sb);                           // [32][WS] window byte offsets
+    unsigned char *winb = smr + 2 * sb + 32 * WS * 4 + w * WR * kRowBytes;  // this warp's window
+    const unsigned wbase = (unsigned)__cvta_generic_to_shared(winb) + 16u * kv;  // this lane's vector
+#ifdef SPK_DEVICE_CHECKS
+    const unsigned wb = (unsigned)(WR * kRowBytes);
+#endif
     const ChainTask t = A.tasks[blockIdx.x];
     const int n = A.n;
+    const int c0 = RPW * w;
+    const int nkw = max(0, min(RPW, A.nk - c0));
     // window: the coupling rows above the task (phase 4: x from phase 1; phase
     // 1: zero); farther rows start at zero, so that no stale value is ever read
-    for (int i = lane; i < WR; i += 32) {
+    for (int e = lane; e < WR * RPW; e += 32) {
+        const int i = e / RPW, k = e % RPW;
         const int r = t.hi + i;
-        const bool ok = PRE && r < n && i < A.reach;
+        const bool ok = PRE && r < n && i < A.reach && k < nkw;
         const long long o = A.rev ? (long long)n - 1 - r : r;
-        T *wr = win + (r % WR) * kRhsPad;
-        for (int k = 0; k < 32; k++) wr[k] = (ok && k < A.nk) ? (T)A.X[k * A.ldx + CK(o, n, 36)] : T(0);
+        T *wr = (T *)(winb + (r % WR) * kRowBytes);
+        wr[k] = ok ? (T)A.X[(long long)(c0 + k) * A.ldx + CK(o, n, 36)] : T(0);
     }
+    // this lane's right-hand sides b[r][c0 + V kv + e] (0 outside the task or past nk)
+    auto bload = [&](int r, double *bv) {
+        const bool in = r >= t.lo && r < t.hi;
+        const long long o = A.rev ? (long long)n - 1 - r : r;
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const int c = V * kv + e;
+            bv[e] = (in && c < nkw) ? A.B[(long long)(c0 + c) * A.ldb + CK(o, n, 35)] : 0.0;
+        }
+    };
     const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
+    double bn[V];  // the next group's right-hand sides (loaded a group ahead of use)
+    bload(((t.hi - 1 - 32 * jt) | 3) + 32 * jt - q, bn);
     auto tile_ptr = [&](int jj, int &p0, int &wq) {
         p0 = __ldg(A.ptr + CK(jj, A.nptr, 37));
         wq = (__ldg(A.ptr + CK(jj + 1, A.nptr, 38)) - p0) >> 5;
     };
     int p0n, wqn;
     tile_ptr(jt, p0n, wqn);
-    rhs_stage_tile<T, W>(A, rhs_stage<T>(smr, A.sw), jt, p0n, wqn, t.lo, t.hi, lane);
+    rhs_stage_tile<T, W>(A, rhs_stage<T>(smr, A.sw), jt, p0n, wqn, t.lo, t.hi, lane, w, nw);
     cpa_commit();
     int wq_cur = wqn;
     if (jt - 1 >= jb) tile_ptr(jt - 1, p0n, wqn);
     for (int j = jt, it = 0; j >= jb; j--, it++) {
         const RhsStage<T> S = rhs_stage<T>(smr + (it & 1) * sb, A.sw);
         const int wq = wq_cur;
+        __syncthreads();  // every warp is done with the other buffer and with wi
         if (j - 1 >= jb) {
-            rhs_stage_tile<T, W>(A, rhs_stage<T>(smr + ((it + 1) & 1) * sb, A.sw), j - 1, p0n, wqn, t.lo, t.hi, lane);
+            rhs_stage_tile<T, W>(A, rhs_stage<T>(smr + ((it + 1) & 1) * sb, A.sw), j - 1, p0n, wqn, t.lo, t.hi, lane,
+                                 w, nw);
             wq_cur = wqn;
             if (j - 2 >= jb) tile_ptr(j - 2, p0n, wqn);
         }
         cpa_commit();
         cpa_wait<1>();
+        __syncthreads();  // tile j has landed, every thread's copies
         const int row0 = 32 * j;
         const int base = row0 % WR;
-        // this lane's row: window element index of every slot's column
-        {
-            unsigned words[W / 2];
+        auto slot_of = [&](int i) {
+            const int v = base + i;
+            return v >= WR ? v - WR : v;
+        };
+        // lane = row i: the window byte offset of every slot's column (warp w
+        // takes the offset words k4 with k4 % nw == w; four slots a word)
 #pragma unroll
-            for (int k4 = 0; k4 < W / 4; k4++) {
-                const unsigned ow = 4 * k4 < wq ? S.o[32 * k4 + lane] : 0u;
+        for (int k4 = 0; k4 < WS / 4; k4++) {
+            if (k4 % nw == w) {
+                const unsigned ow = (k4 < W / 4 && 4 * k4 < wq) ? S.o[32 * k4 + lane] : 0u;
+                unsigned bo[4];
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    unsigned pr = 0;
-#pragma unroll
-                    for (int u = 0; u < 2; u++) {
-                        int v = base + lane + (int)((ow >> (8 * (2 * h + u))) & 0xff);
-                        v -= v >= WR ? WR : 0;
-                        v -= v >= WR ? WR : 0;
-                        v -= v >= WR ? WR : 0;
-                        pr |= (unsigned)(v * kRhsPad * (int)sizeof(T)) << (16 * u);  // byte offset
-                    }
-                    words[2 * k4 + h] = pr;
+                for (int u = 0; u < 4; u++) {
+                    int v = base + lane + (int)((ow >> (8 * u)) & 0xff);
+                    v -= v >= WR ? WR : 0;
+                    v -= v >= WR ? WR : 0;
+                    v -= v >= WR ? WR : 0;
+                    bo[u] = (unsigned)(v * kRowBytes);
                 }
-            }
-            // every word, so that the slots past the tile's width (own row,
-            // weight zero below) index the window
-#pragma unroll
-            for (int k = 0; k < W / 2; k++) wi[lane * WIP + k] = words[k];
-            // a half-filled group of eight slots: zero weights for its second half
-            if (wq & 4) {
-                S.v[CK(64 * (wq >> 1) + 2 * lane, 32 * A.sw, 39)] = T(0);
-                S.v[CK(64 * (wq >> 1) + 2 * lane + 1, 32 * A.sw, 39)] = T(0);
-                S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane, 32 * A.sw, 40)] = T(0);
-                S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane + 1, 32 * A.sw, 40)] = T(0);
+                *reinterpret_cast<uint4 *>(wi + lane * WS + 4 * k4) = make_uint4(bo[0], bo[1], bo[2], bo[3]);
             }
         }
-        __syncwarp();  // every lane's copies and indices are visible to the warp
+        // a half-filled group of eight slots: zero weights for its second half
+        if (w == 0 && (wq & 4)) {
+            S.v[CK(64 * (wq >> 1) + 2 * lane, 32 * A.sw, 39)] = T(0);
+            S.v[CK(64 * (wq >> 1) + 2 * lane + 1, 32 * A.sw, 39)] = T(0);
+            S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane, 32 * A.sw, 40)] = T(0);
+            S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane + 1, 32 * A.sw, 40)] = T(0);
+        }
+        __syncthreads();  // offsets and zeroed weights are visible to every warp
         const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
-        const char *wl = (const char *)(win + lane);  // this lane's column of the window
-        for (int r = a1 - 1; r >= a0; r--) {
-            const int i = r - row0;
-            T acc = (T)S.b[i * kRhsPad + lane] * S.rd[i];
-            T p[2] = {T(0), T(0)};
-            // groups of four slot pairs, branch-free inside (the second half of a
-            // half-filled group has weight zero)
+        // groups of four rows, top first; lane (q, kv) solves the row at place q
+        // for its V right-hand sides; rows below a0 are computed but not stored
+        for (int top = (a1 - 1 - row0) | 3; top >= a0 - row0; top -= 4) {
+            const int i = top - q;
+            double bv[V];
+#pragma unroll
+            for (int e = 0; e < V; e++) bv[e] = bn[e];
+            bload(row0 + i - 4, bn);
+            const T rd = S.rd[i];
+            T acc[4][V];
+#pragma unroll
+            for (int e = 0; e < V; e++) {
+                acc[0][e] = acc[1][e] = acc[2][e] = acc[3][e] = T(0);
+            }
 #pragma unroll
             for (int g = 0; g < (W + 7) / 8; g++) {
                 if (8 * g < wq) {
+                    // eight slots: offsets, then the window loads, then the sums
+                    constexpr int NS = W < 8 ? W : 8;
+                    unsigned oa[8];
+                    const uint4 a4 = *reinterpret_cast<const uint4 *>(wi + i * WS + 8 * g);
+                    oa[0] = a4.x; oa[1] = a4.y; oa[2] = a4.z; oa[3] = a4.w;
+                    if (NS > 4) {
+                        const uint4 a5 = *reinterpret_cast<const uint4 *>(wi + i * WS + 8 * g + 4);
+                        oa[4] = a5.x; oa[5] = a5.y; oa[6] = a5.z; oa[7] = a5.w;
+                    }
+                    VT xv[8];
 #pragma unroll
-                    for (int h = 0; h < 4; h++) {
-                        const int k = 4 * g + h;
-                        if (2 * k < W) {
-                            const V2 v2 = *reinterpret_cast<const V2 *>(S.v + CK(64 * k + 2 * i, 32 * A.sw - 1, 41));
-                            const unsigned w2 = wi[i * WIP + k];
-                            const int wb = WR * kRhsPad * (int)sizeof(T);
-                            p[0] = fma(v2.x, *reinterpret_cast<const T *>(wl + CK(w2 & 0xffffu, wb, 42)), p[0]);
-                            p[1] = fma(v2.y, *reinterpret_cast<const T *>(wl + CK(w2 >> 16, wb, 43)), p[1]);
+                    for (int u = 0; u < NS; u++) xv[u] = lds_v(wbase + CK(oa[u], wb, 42), VT{});
+#pragma unroll
+                    for (int hh = 0; hh < NS / 2; hh++) {
+                        const V2 vv = *reinterpret_cast<const V2 *>(S.v + CK(64 * (4 * g + hh) + 2 * i, 32 * A.sw - 1, 41));
+                        const T *xa = reinterpret_cast<const T *>(&xv[2 * hh]);
+                        const T *xb = reinterpret_cast<const T *>(&xv[2 * hh + 1]);
+#pragma unroll
+                        for (int e = 0; e < V; e++) {
+                            acc[(2 * hh) & 3][e] = fma(vv.x, xa[e], acc[(2 * hh) & 3][e]);
+                            acc[(2 * hh + 1) & 3][e] = fma(vv.y, xb[e], acc[(2 * hh + 1) & 3][e]);
                         }
                     }
                 }
             }
-            int slot = base + i;
-            slot -= slot >= WR ? WR : 0;
-            win[slot * kRhsPad + lane] = acc - (p[0] + p[1]);
+            VT xr;
+            T *x = reinterpret_cast<T *>(&xr);
+#pragma unroll
+            for (int e = 0; e < V; e++) x[e] = (T)bv[e] * rd - ((acc[0][e] + acc[1][e]) + (acc[2][e] + acc[3][e]));
+            // the in-group chain: step d hands place d's values to the lanes
+            // below it; rows at or above a1 (a task's first group only) keep
+            // their window value, the group's lowest row is always below a1
+            const unsigned ad = wbase + (unsigned)(slot_of(i) * kRowBytes);
+            const int r = row0 + i;
+            const bool first = row0 + top >= a1;
+            T c3[3];
+            {
+                const VT n0 = *reinterpret_cast<const VT *>(S.nr + 4 * i);
+                c3[0] = reinterpret_cast<const T *>(&n0)[0];
+                c3[1] = reinterpret_cast<const T *>(&n0)[1];
+                if (sizeof(T) == 8) c3[2] = S.nr[4 * i + 2];
+                else c3[2] = reinterpret_cast<const T *>(&n0)[2];
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                if (first && q == d && r >= a1) xr = lds_v(ad, VT{});
+                VT bd;
+                T *bdt = reinterpret_cast<T *>(&bd);
+                const T *xs = reinterpret_cast<const T *>(&xr);
+#pragma unroll
+                for (int e = 0; e < V; e++) bdt[e] = __shfl_sync(0xffffffffu, xs[e], kv + 8 * d);
+                if (q > d) {
+#pragma unroll
+                    for (int e = 0; e < V; e++) x[e] = fma(-c3[d], bdt[e], x[e]);
+                }
+            }
+            if (r >= a0 && r < a1) {
+                sts_v(ad, xr);
+                // one warp: x straight from the row loop (four rows of a column
+                // per 32-byte sector); two warps share the load/store path, and
+                // the tile's transpose below keeps their stores coalesced
+                if (nw == 1 && r >= t.st_lo && r < t.st_hi) {
+                    const long long o = A.rev ? (long long)n - 1 - r : r;
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if (V * kv + e < nkw)
+                            A.X[(long long)(c0 + V * kv + e) * A.ldx + CK(o, n, 44)] = (double)x[e];
+                }
+            }
         }
-        __syncwarp();
-        // x rows of this tile out (lane = row), for the rows this task stores
-        {
+        if (nw > 1) {
+            __syncwarp();
+            // x rows of this tile out (lane = row), one 16-byte vector per load
             const int r = row0 + lane;
             if (r >= a0 && r < a1 && r >= t.st_lo && r < t.st_hi) {
                 const long long o = A.rev ? (long long)n - 1 - r : r;
-                int slot = base + lane;
-                slot -= slot >= WR ? WR : 0;
-                const T *wr = win + slot * kRhsPad;
-                for (int k = 0; k < A.nk; k++) A.X[k * A.ldx + CK(o, n, 44)] = (double)wr[k];
+                const unsigned ar = (unsigned)__cvta_generic_to_shared(winb) + (unsigned)(slot_of(lane) * kRowBytes);
+                for (int k0 = 0; k0 < nkw; k0 += V) {
+                    const VT val = lds_v(ar + 16u * (k0 / V), VT{});
+                    const T *vt = reinterpret_cast<const T *>(&val);
+#pragma unroll
+                    for (int e = 0; e < V; e++)
+                        if (k0 + e < nkw) A.X[(long long)(c0 + k0 + e) * A.ldx + CK(o, n, 44)] = (double)vt[e];
+                }
             }
         }
     }
     cpa_wait<0>();
 }
 
-size_t rhs_smem_bytes(const spk_system *s, int tsize) {
-    const int W = s->ch_width;
-    return 2 * (size_t)rhs_stage_bytes(s->ch_sw, tsize) + ((32 * (W / 2 + 1) * 4 + 15) & ~15) +
-           (size_t)tsize * (s->ch_reach + 32) * kRhsPad;
+size_t rhs_smem_bytes(const spk_system *s, int tsize, int nw) {
+    return 2 * (size_t)rhs_stage_bytes(s->ch_sw, tsize) + 32 * rhs_wi_stride(s->ch_width) * 4 +
+           (size_t)nw * kRowBytes * (s->ch_reach + 32);
 }
 
 template <typename T, bool PRE>
 int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, const double *B, long long ldb,
                      double *X, long long ldx, cudaStream_t st) {
     if (ntasks <= 0) return SPK_OK;
+    const bool f64 = sizeof(T) == 8;
     RhsArgs<T> A;
     A.tasks = tasks;
-    A.val = sizeof(T) == 8 ? (const T *)(const void *)s->ch_val.p : (const T *)(const void *)s->ch_valf.p;
+    A.val = f64 ? (const T *)(const void *)s->ch_valb.p : (const T *)(const void *)s->ch_valbf.p;
+    A.near = f64 ? (const T *)(const void *)s->ch_near.p : (const T *)(const void *)s->ch_nearf.p;
     A.off = (const unsigned *)s->ch_off.p;
     A.ptr = s->ch_ptr.p;
-    A.rd = sizeof(T) == 8 ? (const T *)(const void *)s->rdiag.p : (const T *)(const void *)s->rdiagf.p;
+    A.rd = f64 ? (const T *)(const void *)s->rdiag.p : (const T *)(const void *)s->rdiagf.p;
     A.n = s->n;
     A.B = B;
     A.ldb = ldb;
@@ -744,18 +909,20 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
     A.sw = s->ch_sw;
     A.nval = (long long)s->ch_val.n;
     A.nptr = (long long)s->ch_ptr.n;
-    A.nrd = (long long)(sizeof(T) == 8 ? s->rdiag.n : s->rdiagf.n);
+    A.nrd = (long long)(f64 ? s->rdiag.n : s->rdiagf.n);
+    A.nnear = (long long)s->ch_near.n;
     A.err = s->d_err.p;
     A.fail_entry = s->dbg_fail_waits > 0;
-    const int W = s->ch_width;
-    const size_t smem = rhs_smem_bytes(s, sizeof(T));
+    const int rpw = 8 * (16 / (int)sizeof(T));  // right-hand sides per warp
+    const int nw = (nk + rpw - 1) / rpw;
+    const size_t smem = rhs_smem_bytes(s, sizeof(T), nw);
     auto go = [&](auto kern) -> int {
         SPK_TRY(allow_smem(kern));
-        kern<<<ntasks, 32, smem, st>>>(A);
+        kern<<<ntasks, 32 * nw, smem, st>>>(A);
         SPK_CUDA(cudaGetLastError());
         return SPK_OK;
     };
-    switch (W) {
+    switch (s->ch_width) {
         case 4: SPK_TRY(go(k_chain_rhs<T, 4, PRE>)); break;
         case 8: SPK_TRY(go(k_chain_rhs<T, 8, PRE>)); break;
         case 16: SPK_TRY(go(k_chain_rhs<T, 16, PRE>)); break;
@@ -818,23 +985,40 @@ __global__ void k_chain_to_float(long long n, const double *__restrict__ a, floa
 }
 
 // FP32 copies of the chain values and of 1/diagonal (made on first use)
-int chain_fp32(spk_system *s) {
-    if (s->ch_valf.p) return SPK_OK;
-    SPK_TRY(s->ch_valf.alloc(s->ch_val.n));
-    if (!s->rdiagf.p) {
-        SPK_TRY(s->rdiagf.alloc(s->rdiag.n));
-        k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->rdiag.n, s->rdiag.p, s->rdiagf.p);
+// The batched kernel's slot values and near coefficients (FP64, and FP32 when
+// fp32), made on the first batched solve that needs them.
+int chain_batch_values(spk_system *s, int fp32) {
+    if (!s->ch_valb.p) {
+        const long long rows = 32ll * ((long long)s->ch_ptr.n - 1);
+        SPK_TRY(s->ch_valb.alloc(s->ch_val.n));
+        SPK_TRY(s->ch_near.alloc(std::max(4 * rows, 4ll)));
+        k_chain_near<<<(unsigned)((rows + 255) / 256), 256, 0, s->stream>>>(
+            rows, s->ch_ptr.p, s->ch_val.p, (const unsigned *)s->ch_off.p, s->ch_valb.p, s->ch_near.p);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaStreamSynchronize(s->stream));
     }
-    k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->ch_val.n, s->ch_val.p, s->ch_valf.p);
-    SPK_CUDA(cudaGetLastError());
-    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    if (fp32 && !s->ch_valbf.p) {
+        SPK_TRY(s->ch_valbf.alloc(s->ch_valb.n));
+        SPK_TRY(s->ch_nearf.alloc(s->ch_near.n));
+        if (!s->rdiagf.p) {
+            SPK_TRY(s->rdiagf.alloc(s->rdiag.n));
+            k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->rdiag.n, s->rdiag.p, s->rdiagf.p);
+        }
+        k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->ch_valb.n, s->ch_valb.p, s->ch_valbf.p);
+        k_chain_to_float<<<1184, 256, 0, s->stream>>>((long long)s->ch_near.n, s->ch_near.p, s->ch_nearf.p);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaStreamSynchronize(s->stream));
+    }
     return SPK_OK;
 }
 
 void chain_release(spk_system *s) {
     s->chain_ok = 0;
     s->ch_val.release();
-    s->ch_valf.release();
+    s->ch_valb.release();
+    s->ch_valbf.release();
+    s->ch_near.release();
+    s->ch_nearf.release();
     s->ch_off.release();
     s->ch_ptr.release();
     s->d_ctasks1.release();
@@ -1009,14 +1193,13 @@ int chain_occupancy(spk_system *s, int *occ) {
 
 // Resident blocks per SM of the batched (FP64) chain kernel.
 int chain_rhs_occupancy(spk_system *s, int *occ) {
-    const int W = s->ch_width;
-    const size_t smem = rhs_smem_bytes(s, sizeof(double));
+    const size_t smem = rhs_smem_bytes(s, sizeof(double), 2);
     auto q = [&](auto kern) -> int {
         SPK_TRY(allow_smem(kern));
-        SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 32, smem));
+        SPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, kern, 64, smem));
         return SPK_OK;
     };
-    switch (W) {
+    switch (s->ch_width) {
         case 4: return q(k_chain_rhs<double, 4, false>);
         case 8: return q(k_chain_rhs<double, 8, false>);
         case 16: return q(k_chain_rhs<double, 16, false>);
@@ -1131,8 +1314,8 @@ int chain_solve_rhs(spk_system *s, int fp32, int nk, const double *B, long long 
     const bool own = bp.len > 0;  // the batched kernel's own chains
     const ChainTask *t1 = own ? bp.d1.p : s->d_ctasks1.p, *t4 = own ? bp.d4.p : s->d_ctasks4.p;
     const int n1 = own ? (int)bp.h1.size() : s->nctasks1, n4 = own ? (int)bp.h4.size() : s->nctasks4;
+    SPK_TRY(chain_batch_values(s, fp32));
     if (fp32) {
-        SPK_TRY(chain_fp32(s));
         SPK_TRY((launch_chain_rhs<float, false>(s, t1, n1, nk, B, ldb, X, ldx, st)));
         SPK_TRY((launch_chain_rhs<float, true>(s, t4, n4, nk, B, ldb, X, ldx, st)));
     } else {

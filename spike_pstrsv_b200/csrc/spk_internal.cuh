@@ -171,7 +171,10 @@ struct spk_system {
     // chain solver (default one-right-hand-side solve; chain.cu)
     int chain_ok = 0, ch_width = 0, ch_sw = 0, ch_reach = 0, ch_win = 0, ch_count = 0, ch_len = 0, ch_stages = 3;
     spk::DBuf<double> ch_val;          // row-scaled off-diagonals, sliced ELL
-    spk::DBuf<float> ch_valf;          // their FP32 copy (batched FP32 solves, made on first use)
+    spk::DBuf<double> ch_valb;         // batched solves: the same with in-group coefficients zeroed
+    spk::DBuf<float> ch_valbf;         //   and its FP32 copy (made on first use)
+    spk::DBuf<double> ch_near;         // batched solves: [rows][4] in-group coefficients
+    spk::DBuf<float> ch_nearf;         //   and its FP32 copy
     spk::DBuf<unsigned char> ch_off;   // column offsets c - r (8 bits)
     spk::DBuf<int> ch_ptr;             // first slot of each 32-row tile
     spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;

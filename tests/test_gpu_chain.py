@@ -158,3 +158,29 @@ def test_chain_batched_matches_substitution(monkeypatch, uplo, nrhs):
     assert resid <= 1e-12 and it >= 1
     X = dX.cpu().numpy()
     assert max(rel_err(X[k], Xt[k]) for k in range(nrhs)) <= TOL
+
+
+@pytest.mark.parametrize("per_row,band,m", [(1, 8, 70001), (3, 16, 65539), (7, 128, 90013),
+                                            (24, 100, 100003), (33, 64, 200003)])
+def test_chain_batched_widths(monkeypatch, per_row, band, m):
+    """The batched chain kernel at every slot width (4 to 64 slots per tile),
+    reach up to 128 and row counts that are not a multiple of the 32-row tile
+    (so a task's first tile starts part-way), FP64 against the substitution."""
+    import torch
+
+    monkeypatch.setenv("SPK_CHAIN_BATCH", "1")
+    L = synth.banded_lower(m, per_row=per_row, band=band, seed=per_row)
+    for uplo in ("L", "U"):
+        A = L if uplo == "L" else synth.transpose(L)
+        Xt, B = synth.make_rhs(A, seed=3, nrhs=7)
+        S = gpu_system(A, 16, uplo)
+        assert S.scalar("chain") == 1
+        dB = torch.from_numpy(B).cuda()
+        dX = torch.zeros_like(dB)
+        S.solve_batch(dB, dX, mode=0)
+        X = dX.cpu().numpy()
+        for k in (0, 3, 6):
+            assert rel_err(X[k], oracle.sequential_solve(A, B[k], uplo)) <= TOL, (uplo, k)
+        assert max(rel_err(X[k], Xt[k]) for k in range(7)) <= TOL
+        # the single solve (lane = row kernel) agrees to rounding
+        assert rel_err(S.solve(B[2]), X[2]) <= 1e-14
