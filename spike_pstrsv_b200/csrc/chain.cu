@@ -526,12 +526,11 @@ int launch_chain(spk_system *s, const ChainTask *tasks, int ntasks, const double
 // read only rows of earlier groups and run side by side; the chain then hands
 // each place's values to the lanes below it by shuffles (three steps).
 //
-// A tile (32 rows) is staged by cp.async one tile ahead: slot values and
-// offsets, 1/diag and the near coefficients.  When it has landed, each row's
-// offsets become window byte offsets (row of the column mod WR, times 144).
-// Right-hand sides are read straight into registers a group ahead of use;
-// solved rows go to X from the row loop (one warp) or through a transpose of
-// the tile (lane = row, two warps).
+// A tile (32 rows) is staged by cp.async one tile ahead: slot values, offset
+// bytes and 1/diag; the row loop turns a slot's offset into its column's window
+// row.  Right-hand sides and near coefficients are read straight into
+// registers a group ahead of use; solved rows go to X from the row loop (one
+// warp) or through a transpose of the tile (lane = row, two warps).
 
 template <typename T>
 struct RhsArgs {
@@ -578,22 +577,15 @@ __device__ __forceinline__ void sts_v(unsigned a, float4 v) {
 
 constexpr int kRowBytes = 144;  // a window row: 8 vectors of right-hand sides + 1 of padding
 
-// Words of window offsets per row, one per slot: W rounded up to whole 16-byte
-// units, an odd number of them (conflict-free 16-byte stores per quarter warp).
-__host__ __device__ constexpr int rhs_wi_stride(int W) {
-    return 4 * ((W / 4) | 1);
-}
-
 template <typename T>
 struct RhsStage {
     T *v;         // [32 sw] as copied: pair (k/2)*32 + l holds slots k, k+1 of row l
     unsigned *o;  // [8 sw]  offset words (k/4)*32 + l
     T *rd;        // [32]
-    T *nr;        // [32][4] near coefficients
 };
 
 __host__ __device__ __forceinline__ int rhs_stage_bytes(int sw, int tsize) {
-    return 32 * sw * tsize + 32 * sw + 32 * 8 + 128 * tsize;
+    return 32 * sw * tsize + 32 * sw + 32 * 8;
 }
 
 template <typename T>
@@ -602,12 +594,11 @@ __device__ __forceinline__ RhsStage<T> rhs_stage(unsigned char *base, int sw) {
     S.v = (T *)base;
     S.o = (unsigned *)(base + 32 * sw * sizeof(T));
     S.rd = (T *)(base + 32 * sw * sizeof(T) + 32 * sw);
-    S.nr = (T *)(base + 32 * sw * sizeof(T) + 32 * sw + 32 * 8);
     return S;
 }
 
 // cp.async of tile j: warp w copies the slot pairs k with k % nw == w (lane =
-// row); warp 0 also 1/diag and the near coefficients of the task's rows.
+// row); warp 0 also 1/diag of the task's rows.
 template <typename T, int W>
 __device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsStage<T> &S, int j, int p0, int wq,
                                                int lo, int hi, int lane, int w, int nw) {
@@ -628,8 +619,6 @@ __device__ __forceinline__ void rhs_stage_tile(const RhsArgs<T> &A, const RhsSta
     if (w == 0 && r >= lo && r < hi) {
         if (sizeof(T) == 8) cpa8(S.rd + lane, A.rd + CK(r, A.nrd, 34));
         else cpa4(S.rd + lane, A.rd + CK(r, A.nrd, 34));
-        for (int c = 0; c < 4 * (int)sizeof(T); c += 16)
-            cpa16((char *)(S.nr + 4 * lane) + c, (const char *)(A.near + CK(4ll * r, A.nnear - 3, 46)) + c);
     }
 }
 
@@ -674,7 +663,6 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
     using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;  // 16 bytes
     constexpr int V = 16 / (int)sizeof(T);  // right-hand sides per lane
     constexpr int RPW = 8 * V;              // right-hand sides per warp
-    constexpr int WS = rhs_wi_stride(W);    // window offsets per row (words, one per slot)
     extern __shared__ __align__(16) unsigned char smr[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, nw = blockDim.x >> 5;
     const int q = lane >> 3, kv = lane & 7;  // place in the group of four, vector of right-hand sides
@@ -684,8 +672,7 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
     }
     const int WR = A.wr;
     const int sb = rhs_stage_bytes(A.sw, sizeof(T));
-    unsigned *wi = (unsigned *)(smr + 2 * sb);                           // [32][WS] window byte offsets
-    unsigned char *winb = smr + 2 * sb + 32 * WS * 4 + w * WR * kRowBytes;  // this warp's window
+    unsigned char *winb = smr + 2 * sb + w * WR * kRowBytes;  // this warp's window
     const unsigned wbase = (unsigned)__cvta_generic_to_shared(winb) + 16u * kv;  // this lane's vector
 #ifdef SPK_DEVICE_CHECKS
     const unsigned wb = (unsigned)(WR * kRowBytes);
@@ -715,8 +702,30 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
         }
     };
     const int jt = (t.hi - 1) >> 5, jb = t.lo >> 5;
-    double bn[V];  // the next group's right-hand sides (loaded a group ahead of use)
-    bload(((t.hi - 1 - 32 * jt) | 3) + 32 * jt - q, bn);
+    // this lane's row's in-group coefficients (0 outside the task)
+    auto nload = [&](int r, T *c) {
+        if (r >= t.lo && r < t.hi) {
+            const VT *np = reinterpret_cast<const VT *>(A.near + CK(4ll * r, A.nnear - 3, 46));
+            const VT u0 = np[0];
+            c[0] = reinterpret_cast<const T *>(&u0)[0];
+            c[1] = reinterpret_cast<const T *>(&u0)[1];
+            if (sizeof(T) == 8) {
+                const VT u1 = np[1];
+                c[2] = reinterpret_cast<const T *>(&u1)[0];
+            } else {
+                c[2] = reinterpret_cast<const T *>(&u0)[2];
+            }
+        } else {
+            c[0] = c[1] = c[2] = T(0);
+        }
+    };
+    double bn[V];  // the next group's right-hand sides and coefficients (loaded a group ahead of use)
+    T cn[3];
+    {
+        const int r0 = ((t.hi - 1 - 32 * jt) | 3) + 32 * jt - q;
+        bload(r0, bn);
+        nload(r0, cn);
+    }
     auto tile_ptr = [&](int jj, int &p0, int &wq) {
         p0 = __ldg(A.ptr + CK(jj, A.nptr, 37));
         wq = (__ldg(A.ptr + CK(jj + 1, A.nptr, 38)) - p0) >> 5;
@@ -730,7 +739,7 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
     for (int j = jt, it = 0; j >= jb; j--, it++) {
         const RhsStage<T> S = rhs_stage<T>(smr + (it & 1) * sb, A.sw);
         const int wq = wq_cur;
-        __syncthreads();  // every warp is done with the other buffer and with wi
+        __syncthreads();  // every warp is done with the other buffer
         if (j - 1 >= jb) {
             rhs_stage_tile<T, W>(A, rhs_stage<T>(smr + ((it + 1) & 1) * sb, A.sw), j - 1, p0n, wqn, t.lo, t.hi, lane,
                                  w, nw);
@@ -746,32 +755,6 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
             const int v = base + i;
             return v >= WR ? v - WR : v;
         };
-        // lane = row i: the window byte offset of every slot's column (warp w
-        // takes the offset words k4 with k4 % nw == w; four slots a word)
-#pragma unroll
-        for (int k4 = 0; k4 < WS / 4; k4++) {
-            if (k4 % nw == w) {
-                const unsigned ow = (k4 < W / 4 && 4 * k4 < wq) ? S.o[32 * k4 + lane] : 0u;
-                unsigned bo[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    int v = base + lane + (int)((ow >> (8 * u)) & 0xff);
-                    v -= v >= WR ? WR : 0;
-                    v -= v >= WR ? WR : 0;
-                    v -= v >= WR ? WR : 0;
-                    bo[u] = (unsigned)(v * kRowBytes);
-                }
-                *reinterpret_cast<uint4 *>(wi + lane * WS + 4 * k4) = make_uint4(bo[0], bo[1], bo[2], bo[3]);
-            }
-        }
-        // a half-filled group of eight slots: zero weights for its second half
-        if (w == 0 && (wq & 4)) {
-            S.v[CK(64 * (wq >> 1) + 2 * lane, 32 * A.sw, 39)] = T(0);
-            S.v[CK(64 * (wq >> 1) + 2 * lane + 1, 32 * A.sw, 39)] = T(0);
-            S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane, 32 * A.sw, 40)] = T(0);
-            S.v[CK(64 * ((wq >> 1) + 1) + 2 * lane + 1, 32 * A.sw, 40)] = T(0);
-        }
-        __syncthreads();  // offsets and zeroed weights are visible to every warp
         const int a0 = max(t.lo, row0), a1 = min(t.hi, row0 + 32);
         // groups of four rows, top first; lane (q, kv) solves the row at place q
         // for its V right-hand sides; rows below a0 are computed but not stored
@@ -781,36 +764,45 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
 #pragma unroll
             for (int e = 0; e < V; e++) bv[e] = bn[e];
             bload(row0 + i - 4, bn);
+            T c3[3] = {cn[0], cn[1], cn[2]};
+            nload(row0 + i - 4, cn);
             const T rd = S.rd[i];
             T acc[4][V];
 #pragma unroll
             for (int e = 0; e < V; e++) {
                 acc[0][e] = acc[1][e] = acc[2][e] = acc[3][e] = T(0);
             }
+            const int si = slot_of(i);  // window row of this lane's row
 #pragma unroll
             for (int g = 0; g < (W + 7) / 8; g++) {
                 if (8 * g < wq) {
-                    // eight slots: offsets, then the window loads, then the sums
+                    // eight slots (four in a half-filled group: the tile's slot
+                    // count is a multiple of four): offsets, window loads, sums
                     constexpr int NS = W < 8 ? W : 8;
-                    unsigned oa[8];
-                    const uint4 a4 = *reinterpret_cast<const uint4 *>(wi + i * WS + 8 * g);
-                    oa[0] = a4.x; oa[1] = a4.y; oa[2] = a4.z; oa[3] = a4.w;
-                    if (NS > 4) {
-                        const uint4 a5 = *reinterpret_cast<const uint4 *>(wi + i * WS + 8 * g + 4);
-                        oa[4] = a5.x; oa[5] = a5.y; oa[6] = a5.z; oa[7] = a5.w;
-                    }
+                    const bool full = 8 * g + 8 <= wq;
+                    unsigned ow[2];
+                    ow[0] = S.o[CK(64 * g + i, 8 * A.sw, 47)];
+                    ow[1] = (NS > 4 && full) ? S.o[CK(64 * g + 32 + i, 8 * A.sw, 47)] : 0u;
                     VT xv[8];
 #pragma unroll
-                    for (int u = 0; u < NS; u++) xv[u] = lds_v(wbase + CK(oa[u], wb, 42), VT{});
+                    for (int u = 0; u < NS; u++) {
+                        if (u < 4 || full) {
+                            int v = si + (int)((ow[u >> 2] >> (8 * (u & 3))) & 0xff);
+                            v -= v >= WR ? WR : 0;
+                            xv[u] = lds_v(wbase + CK((unsigned)(v * kRowBytes), wb, 42), VT{});
+                        }
+                    }
 #pragma unroll
                     for (int hh = 0; hh < NS / 2; hh++) {
-                        const V2 vv = *reinterpret_cast<const V2 *>(S.v + CK(64 * (4 * g + hh) + 2 * i, 32 * A.sw - 1, 41));
-                        const T *xa = reinterpret_cast<const T *>(&xv[2 * hh]);
-                        const T *xb = reinterpret_cast<const T *>(&xv[2 * hh + 1]);
+                        if (hh < 2 || full) {
+                            const V2 vv = *reinterpret_cast<const V2 *>(S.v + CK(64 * (4 * g + hh) + 2 * i, 32 * A.sw - 1, 41));
+                            const T *xa = reinterpret_cast<const T *>(&xv[2 * hh]);
+                            const T *xb = reinterpret_cast<const T *>(&xv[2 * hh + 1]);
 #pragma unroll
-                        for (int e = 0; e < V; e++) {
-                            acc[(2 * hh) & 3][e] = fma(vv.x, xa[e], acc[(2 * hh) & 3][e]);
-                            acc[(2 * hh + 1) & 3][e] = fma(vv.y, xb[e], acc[(2 * hh + 1) & 3][e]);
+                            for (int e = 0; e < V; e++) {
+                                acc[(2 * hh) & 3][e] = fma(vv.x, xa[e], acc[(2 * hh) & 3][e]);
+                                acc[(2 * hh + 1) & 3][e] = fma(vv.y, xb[e], acc[(2 * hh + 1) & 3][e]);
+                            }
                         }
                     }
                 }
@@ -825,14 +817,6 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
             const unsigned ad = wbase + (unsigned)(slot_of(i) * kRowBytes);
             const int r = row0 + i;
             const bool first = row0 + top >= a1;
-            T c3[3];
-            {
-                const VT n0 = *reinterpret_cast<const VT *>(S.nr + 4 * i);
-                c3[0] = reinterpret_cast<const T *>(&n0)[0];
-                c3[1] = reinterpret_cast<const T *>(&n0)[1];
-                if (sizeof(T) == 8) c3[2] = S.nr[4 * i + 2];
-                else c3[2] = reinterpret_cast<const T *>(&n0)[2];
-            }
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 if (first && q == d && r >= a1) xr = lds_v(ad, VT{});
@@ -881,8 +865,7 @@ __global__ void __launch_bounds__(64) k_chain_rhs(RhsArgs<T> A) {
 }
 
 size_t rhs_smem_bytes(const spk_system *s, int tsize, int nw) {
-    return 2 * (size_t)rhs_stage_bytes(s->ch_sw, tsize) + 32 * rhs_wi_stride(s->ch_width) * 4 +
-           (size_t)nw * kRowBytes * (s->ch_reach + 32);
+    return 2 * (size_t)rhs_stage_bytes(s->ch_sw, tsize) + (size_t)nw * kRowBytes * (s->ch_reach + 32);
 }
 
 template <typename T, bool PRE>
