@@ -246,6 +246,18 @@ long long spk_debug_scalar(const spk_system *s, const char *name);
  * task).  SPK_ERR_STATE unless spk_debug_scalar(s, "chain") == 1. */
 int spk_chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const double *b, double *x, void *stream);
 
+/* Serving residency (no reference counterpart): release every device pool of a
+ * system solved by chains that its solves never read (the CSR copy, the
+ * reference's D / T2 / spike / reduced-system pools, the partition task lists),
+ * keeping the chain layout, 1/diag, the sliced-ELL copy and the chain tasks.
+ * spk_solve, spk_solve_device and spk_solve_batch then always take the chain
+ * kernels; spk_set_truncation, spk_solve_batch_noalloc and group membership
+ * return SPK_ERR_STATE until the system is preprocessed again, and the
+ * released pools read back empty through spk_debug_array.  *freed (may be
+ * NULL) receives the bytes released.  SPK_ERR_STATE unless
+ * spk_debug_scalar(s, "chain") == 1. */
+int spk_compact(spk_system *s, long long *freed);
+
 /* Test hook (no reference counterpart): spk_debug_set(s, "fail_waits", 1) makes
  * every solve kernel of s report a failed bounded wait at entry, before it
  * issues any copy, until the failure has been reported once (SPK_ERR_TIMEOUT
@@ -301,13 +313,14 @@ int spk_server_submit(spk_server *srv, int id, int nrhs, const double *b, double
  * batch's right-hand-side count. */
 int spk_server_wait(spk_server *srv, long long ticket, double *latency_s, double *resid, int *iters,
                     int *batch_rhs);
-/* out[0..14]: resident bytes, staging bytes, resident systems, evictions,
+/* out[0..15]: resident bytes, staging bytes, resident systems, evictions,
  * preprocessings, batches, right-hand sides batched, requests completed, budget,
  * batches retried after releasing idle systems when device memory ran out,
  * batches solved again in FP64 because their scaled residual was above 1e-12
  * (requests still above it fail with SPK_ERR_INPUT), and microseconds spent
  * (summed over the workers) in host staging in, the solves with their device
- * copies, host staging out and preprocessing. */
+ * copies, host staging out and preprocessing, and systems compacted
+ * (spk_compact) to make room before any eviction. */
 int spk_server_stats(spk_server *srv, long long *out, int count);
 
 /* The system used by the Part-1 entry points (NULL before the first preproc). */

@@ -59,6 +59,7 @@ def lib() -> ctypes.CDLL:
         L.spk_debug_scalar.argtypes = [vp, ctypes.c_char_p]
         L.spk_debug_set.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
         L.spk_chain_phase.argtypes = [vp, i, i, i, vp, vp, vp]
+        L.spk_compact.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
         L.spk_legacy_system.restype = vp
         L.spk_set_truncation.argtypes = [vp, d]
         L.spk_check.argtypes = [vp]
@@ -308,6 +309,13 @@ class System:
         device pointers (spk_chain_phase)."""
         _check(lib().spk_chain_phase(self.h, int(phase), int(row_lo), int(row_hi), ctypes.c_void_p(b_ptr),
                                      ctypes.c_void_p(x_ptr), ctypes.c_void_p(stream)))
+
+    def compact(self) -> int:
+        """Release the device pools the chain solves never read (spk_compact);
+        returns the bytes released."""
+        freed = ctypes.c_longlong(0)
+        _check(lib().spk_compact(self.h, ctypes.byref(freed)))
+        return int(freed.value)
 
     def debug_set(self, name: str, value: int) -> "System":
         """Test hooks (spk_debug_set): "fail_waits" makes the solve kernels report a

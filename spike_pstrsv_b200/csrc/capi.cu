@@ -94,6 +94,15 @@ int make_system(spk_system **out) {
         return SPK_ERR_CUDA;
     }
     s->own_stream = 1;
+    // preprocessing's scoped temporaries come from the device's default memory
+    // pool in stream order: keep up to 256 MiB of it mapped between
+    // synchronizations instead of returning it at each one
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        unsigned long long keep = 256ull << 20;  // the attribute is a 64-bit unsigned value
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = s;
     return SPK_OK;
 }
@@ -504,8 +513,57 @@ int spk_set_truncation(spk_system *s, double tau) {
         set_error(SPK_ERR_ARG, "null argument");
         return SPK_ERR_ARG;
     }
+    if (s->lean) {
+        set_error(SPK_ERR_STATE, "the system was compacted (spk_compact): preprocess it again to change the truncation");
+        return SPK_ERR_STATE;
+    }
     s->trunc_tol = tau;
     if (s->built) return solve_prepare(s);
+    return SPK_OK;
+}
+
+int spk_compact(spk_system *s, long long *freed) {
+    if (!s) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!s->built || !s->chain_ok) {
+        set_error(SPK_ERR_STATE, "spk_compact needs a preprocessed system solved by chains");
+        return SPK_ERR_STATE;
+    }
+    if (s->lean) {
+        if (freed) *freed = 0;
+        return SPK_OK;
+    }
+    SPK_TRY(spk::residual_prepare(s));  // diag and ||A|| come from the CSR
+    const long long before = spk_debug_scalar(s, "device_bytes");
+    s->ua.release();
+    s->uia.release();
+    s->uja.release();
+    s->D.release();
+    s->T2.release();
+    s->S.release();
+    s->T.release();
+    s->ID.release();
+    s->JD.release();
+    s->IT2.release();
+    s->JT2.release();
+    s->mapR.release();
+    s->dep.release();
+    s->mapRedX.release();
+    s->IT.release();
+    s->JT.release();
+    s->d_ps.release();
+    s->d_pe.release();
+    s->d_lvl.release();
+    s->d_tasks1.release();
+    s->d_tasks2.release();
+    s->xbuf.release();
+    s->xout_u.release();
+    s->d_red_rows.release();
+    s->d_red_off.release();
+    s->lean = 1;
+    if (freed) *freed = before - spk_debug_scalar(s, "device_bytes");
     return SPK_OK;
 }
 
@@ -530,6 +588,7 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
         return (s->redNec && s->ntasks1 ? 1 : 0) + (s->redNec && s->nkept ? 1 : 0) + 1;
     }
     if (!strcmp(name, "chain")) return s->chain_ok;
+    if (!strcmp(name, "lean")) return s->lean;
     if (!strcmp(name, "device_check")) return chain_device_check();  // checked builds only
     if (!strcmp(name, "chains")) return s->ch_count;
     if (!strcmp(name, "chain_rows")) return s->ch_len;

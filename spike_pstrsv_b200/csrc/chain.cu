@@ -919,13 +919,15 @@ int launch_chain_rhs(spk_system *s, const ChainTask *tasks, int ntasks, int nk, 
 template <typename T>
 int upload_vec(DBuf<T> &d, const std::vector<T> &h) {
     SPK_TRY(d.alloc(h.size()));
-    if (!h.empty()) SPK_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (h.empty()) return SPK_OK;
+    if (d.on_stream) SPK_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, d.ord));
+    else SPK_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
     return SPK_OK;
 }
 
 int spike_firsts(spk_system *s, const std::vector<int2> &chains, std::vector<int> &first) {
-    DBuf<int2> d_ch;
-    DBuf<int> d_first;
+    DBuf<int2> d_ch(s->stream);
+    DBuf<int> d_first(s->stream);
     SPK_TRY(upload_vec(d_ch, chains));
     SPK_TRY(d_first.alloc(chains.size()));
     SpikeArgs A;
@@ -967,7 +969,6 @@ __global__ void k_chain_to_float(long long n, const double *__restrict__ a, floa
         b[i] = (float)a[i];
 }
 
-// FP32 copies of the chain values and of 1/diagonal (made on first use)
 // The batched kernel's slot values and near coefficients (FP64, and FP32 when
 // fp32), made on the first batched solve that needs them.
 int chain_batch_values(spk_system *s, int fp32) {
@@ -1035,7 +1036,7 @@ int chain_prepare(spk_system *s) {
     std::vector<int> hw(ntiles);
     int reach = 0;
     {
-        DBuf<int> width, d_reach;
+        DBuf<int> width(s->stream), d_reach(s->stream);
         SPK_TRY(width.alloc(ntiles));
         SPK_TRY(d_reach.alloc(1));
         SPK_CUDA(cudaMemsetAsync(d_reach.p, 0, sizeof(int), s->stream));

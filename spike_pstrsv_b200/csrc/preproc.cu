@@ -410,7 +410,7 @@ inline int blocks_for(long long n, int bs = 256) { return (int)((n + bs - 1) / b
 int exclusive_scan(const int *in, int *out, int count, cudaStream_t st) {
     size_t tmp = 0;
     SPK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, count, st));
-    DBuf<unsigned char> t;
+    DBuf<unsigned char> t(st);
     SPK_TRY(t.alloc(tmp));
     SPK_CUDA(cub::DeviceScan::ExclusiveSum(t.p, tmp, in, out, count, st));
     return SPK_OK;
@@ -536,6 +536,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         return SPK_ERR_ARG;
     }
     s->built = 0;
+    s->lean = 0;
     // values derived from the previous matrix for the batched solves
     s->ell_valf.release();
     s->rdiagf.release();
@@ -564,7 +565,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     SPK_CUDA(cudaMemsetAsync(s->ua.p + nnz, 0, 16 * sizeof(double), st));
     SPK_CUDA(cudaMemsetAsync(s->uja.p + nnz, 0, 16 * sizeof(int), st));
     {
-        DBuf<double> la; DBuf<int> lia, lja;
+        DBuf<double> la(st); DBuf<int> lia(st), lja(st);
         const double *src_a = a; const int *src_ia = ia, *src_ja = ja;
         if (!on_dev) {
             if (up == 'L') {
@@ -594,7 +595,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     const int *uia = s->uia.p, *uja = s->uja.p;
     const double *ua = s->ua.p;
     {
-        DBuf<unsigned long long> err;
+        DBuf<unsigned long long> err(st);
         SPK_TRY(err.alloc(1));
         SPK_CUDA(cudaMemsetAsync(err.p, 0xff, sizeof(unsigned long long), st));
         k_validate<<<blocks_for(n), 256, 0, st>>>(n, uia, uja, err.p);
@@ -651,7 +652,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     // ---- dependents, interval ends, first dependent rows
     SPK_TRY(s->dep.alloc(n));
     SPK_CUDA(cudaMemsetAsync(s->dep.p, 0, sizeof(int) * n, st));
-    DBuf<int> d_maxIR, d_minDR, d_hasDep;
+    DBuf<int> d_maxIR(st), d_minDR(st), d_hasDep(st);
     {
         std::vector<int> init_max(P), init_min(P);
         for (int t = 0; t < P; t++) { init_max[t] = hps[t] - 1; init_min[t] = hpe[t]; }
@@ -680,15 +681,15 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     // ---- preprocessS_PSTRSV3 (ops.c:214-373)
     s->totalArea = 0;
     int nk = 0;
-    DBuf<int> d_mapR_all;
+    DBuf<int> d_mapR_all(st);
     std::vector<int> colCount(P, 0);
     if (s->redNec) {
         std::vector<char> refl(P, 0);
         for (int t = 1; t < P; t++)
             if (parts[t].minDR < parts[t].pe) refl[t] = 1;
-        DBuf<char> d_refl;
+        DBuf<char> d_refl(st);
         SPK_TRY(to_device(d_refl, refl, st));
-        DBuf<int> cnt, off;
+        DBuf<int> cnt(st), off(st);
         SPK_TRY(cnt.alloc(n + 1));
         SPK_TRY(off.alloc(n + 1));
         SPK_CUDA(cudaMemsetAsync(cnt.p + n, 0, sizeof(int), st));
@@ -699,8 +700,8 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         int nkeys = 0;
         SPK_CUDA(cudaMemcpyAsync(&nkeys, off.p + n, sizeof(int), cudaMemcpyDeviceToHost, st));
         SPK_CUDA(cudaStreamSynchronize(st));
-        DBuf<unsigned long long> keys, sorted, uniq;
-        DBuf<int> nuniq;
+        DBuf<unsigned long long> keys(st), sorted(st), uniq(st);
+        DBuf<int> nuniq(st);
         SPK_TRY(keys.alloc(nkeys));
         SPK_TRY(sorted.alloc(nkeys));
         SPK_TRY(uniq.alloc(nkeys));
@@ -713,18 +714,18 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
             while ((1 << tbits) < P) tbits++;
             size_t tmp = 0;
             SPK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, keys.p, sorted.p, nkeys, 0, 32 + tbits, st));
-            DBuf<unsigned char> tb;
+            DBuf<unsigned char> tb(st);
             SPK_TRY(tb.alloc(tmp));
             SPK_CUDA(cub::DeviceRadixSort::SortKeys(tb.p, tmp, keys.p, sorted.p, nkeys, 0, 32 + tbits, st));
             size_t tmp2 = 0;
             SPK_CUDA(cub::DeviceSelect::Unique(nullptr, tmp2, sorted.p, uniq.p, nuniq.p, nkeys, st));
-            DBuf<unsigned char> tb2;
+            DBuf<unsigned char> tb2(st);
             SPK_TRY(tb2.alloc(tmp2));
             SPK_CUDA(cub::DeviceSelect::Unique(tb2.p, tmp2, sorted.p, uniq.p, nuniq.p, nkeys, st));
             SPK_CUDA(cudaMemcpyAsync(&nk, nuniq.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             SPK_CUDA(cudaStreamSynchronize(st));
         }
-        DBuf<int> d_cc;
+        DBuf<int> d_cc(st);
         SPK_TRY(d_cc.alloc(P));
         SPK_CUDA(cudaMemsetAsync(d_cc.p, 0, sizeof(int) * P, st));
         SPK_TRY(d_mapR_all.alloc(nk));
@@ -768,7 +769,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         if (flb) {
             std::vector<int> hsi(P), hei(P);
             for (int t = 0; t < P; t++) { hsi[t] = parts[t].si; hei[t] = parts[t].ei; }
-            DBuf<int> d_si, d_ei, d_cnt9;
+            DBuf<int> d_si(st), d_ei(st), d_cnt9(st);
             SPK_TRY(to_device(d_si, hsi, st));
             SPK_TRY(to_device(d_ei, hei, st));
             SPK_TRY(d_cnt9.alloc((size_t)P * kLB));
@@ -814,12 +815,12 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         d.flags = ((p.hasRefl || p.isOpt) ? 1 : 0) | (p.hasRefl ? 2 : 0) | (p.hasS ? 4 : 0);
         d.pad = 0;
     }
-    DBuf<PartDev> d_pd;
+    DBuf<PartDev> d_pd(st);
     SPK_TRY(to_device(d_pd, hpd, st));
 
     // ---- D and R_new pools
     {
-        DBuf<int> nD, nR, oR;
+        DBuf<int> nD(st), nR(st), oR(st);
         SPK_TRY(nD.alloc(n + 1));
         SPK_TRY(nR.alloc(n + 1));
         SPK_TRY(oR.alloc(n + 1));
@@ -888,9 +889,9 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
             SPK_TRY(s->T2.alloc(1));
             SPK_TRY(s->JT2.alloc(1));
         } else {
-            DBuf<Seg> d_segs;
+            DBuf<Seg> d_segs(st);
             SPK_TRY(to_device(d_segs, segs, st));
-            DBuf<int> cnt;
+            DBuf<int> cnt(st);
             SPK_TRY(cnt.alloc(row + 1));
             k_t2_counts<<<blocks_for(row + 1), 256, 0, st>>>(row, d_segs.p, (int)segs.size(), s->ID.p, s->JD.p, cnt.p);
             SPK_CUDA(cudaGetLastError());
@@ -941,7 +942,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
             }
         }
         if (!plist.empty()) {
-            DBuf<int> d_pl, d_sd0;
+            DBuf<int> d_pl(st), d_sd0(st);
             SPK_TRY(to_device(d_pl, plist, st));
             SPK_TRY(to_device(d_sd0, sd0, st));
             int bs = std::min(256, ((maxcc + 31) / 32) * 32);
@@ -954,7 +955,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
 
     // ---- reduced system
     {
-        DBuf<int> f, redIdx;
+        DBuf<int> f(st), redIdx(st);
         SPK_TRY(f.alloc(n + 1));
         SPK_TRY(redIdx.alloc(n + 1));
         k_flags<<<blocks_for(n + 1), 256, 0, st>>>(n, s->dep.p, f.p);
@@ -973,7 +974,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
         s->rss = rss;
         SPK_TRY(s->IT.alloc(rss + 1));
         if (rss > 0) {
-            DBuf<int> cnt;
+            DBuf<int> cnt(st);
             SPK_TRY(cnt.alloc(rss + 1));
             k_reduced_rows<<<blocks_for(rss + 1), 256, 0, st>>>(rss, P, dps, d_pd.p, s->mapRedX.p, s->S.p,
                                                                 s->mapR.p, s->dep.p, cnt.p, nullptr, nullptr,

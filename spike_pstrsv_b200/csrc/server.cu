@@ -93,6 +93,7 @@ struct spk_server {
     std::vector<Slot *> slots;
     long long next_ticket = 1, clock = 0;
     long long evictions = 0, preprocs = 0, batches = 0, batched_rhs = 0, completed = 0, nomem_retries = 0;
+    long long compactions = 0;
     long long rechecks = 0;
     // microseconds spent, summed over the workers: host staging in, solve (with
     // the device copies), host staging out, preprocessing
@@ -135,6 +136,21 @@ long long estimate_bytes(const Matrix *M) {
 // Destroy idle resident systems, least recently used first, until `need` more
 // bytes fit.  Called with the lock held; returns whether they fit.
 bool make_room(spk_server *S, long long need, const Matrix *keep) {
+    // first the idle systems solved by chains give up the pools their solves
+    // never read (spk_compact; its releases synchronize the device, so it runs
+    // only when the budget asks for room)
+    for (auto &kv : S->mats) {
+        if (S->resident + S->workspace + need <= S->budget) break;
+        Matrix *M = kv.second;
+        if (M == keep || !M->sys || M->busy) continue;
+        if (spk_debug_scalar(M->sys, "chain") != 1 || spk_debug_scalar(M->sys, "lean") == 1) continue;
+        long long freed = 0;
+        if (spk_compact(M->sys, &freed) == SPK_OK) {
+            S->resident -= freed;
+            M->bytes -= freed;
+            S->compactions++;
+        }
+    }
     while (S->resident + S->workspace + need > S->budget) {
         Matrix *victim = nullptr;
         for (auto &kv : S->mats) {
@@ -515,10 +531,11 @@ int spk_server_stats(spk_server *S, long long *out, int count) {
     std::lock_guard<std::mutex> g(S->mu);
     long long nres = 0;
     for (auto &kv : S->mats) nres += kv.second->sys != nullptr;
-    const long long v[15] = {S->resident,      S->workspace,    nres,           S->evictions,     S->preprocs,
+    const long long v[16] = {S->resident,      S->workspace,    nres,           S->evictions,     S->preprocs,
                              S->batches,       S->batched_rhs,  S->completed,   S->budget,        S->nomem_retries,
-                             S->rechecks,      S->us_in.load(), S->us_solve.load(), S->us_out.load(), S->us_pre.load()};
-    for (int i = 0; i < count && i < 15; i++) out[i] = v[i];
+                             S->rechecks,      S->us_in.load(), S->us_solve.load(), S->us_out.load(), S->us_pre.load(),
+                             S->compactions};
+    for (int i = 0; i < count && i < 16; i++) out[i] = v[i];
     return SPK_OK;
 }
 

@@ -1682,7 +1682,9 @@ __global__ void k_clobber_rhs(int n, int rev, const int *__restrict__ ID, const 
 template <typename T>
 int upload(DBuf<T> &d, const std::vector<T> &h) {
     SPK_TRY(d.alloc(h.size()));
-    if (!h.empty()) SPK_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    if (h.empty()) return SPK_OK;
+    if (d.on_stream) SPK_CUDA(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, d.ord));
+    else SPK_CUDA(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
     return SPK_OK;
 }
 
@@ -1705,8 +1707,8 @@ int solve_prepare(spk_system *s) {
             if (p.hasS && p.nRowsS > 0) plist.push_back(t);
         }
         if (tau >= 0 && !plist.empty()) {
-            DBuf<int> d_pl, d_nr, d_nc, d_first;
-            DBuf<long long> d_ss;
+            DBuf<int> d_pl(s->stream), d_nr(s->stream), d_nc(s->stream), d_first(s->stream);
+            DBuf<long long> d_ss(s->stream);
             SPK_TRY(upload(d_pl, plist));
             SPK_TRY(upload(d_nr, nr));
             SPK_TRY(upload(d_nc, nc));
@@ -1748,12 +1750,12 @@ int solve_prepare(spk_system *s) {
             cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
             if (cols.empty() || cols.size() > 1024) continue;
             const int rows = rl + 1 - p.ps, nc = (int)cols.size();
-            DBuf<int> d_cols, d_first;
-            DBuf<double> W;
+            DBuf<int> d_cols(s->stream), d_first(s->stream);
+            DBuf<double> W(s->stream);
             SPK_TRY(upload(d_cols, cols));
             SPK_TRY(W.alloc((size_t)rows * nc));
             SPK_TRY(d_first.alloc(1));
-            SPK_CUDA(cudaMemcpy(d_first.p, &rows, sizeof(int), cudaMemcpyHostToDevice));
+            SPK_CUDA(cudaMemcpyAsync(d_first.p, &rows, sizeof(int), cudaMemcpyHostToDevice, s->stream));
             k_aux_sweep<<<1, ((nc + 31) / 32) * 32, 0, s->stream>>>(p.ps, rl, p.pe, s->uia.p, s->uja.p, s->ua.p,
                                                                     d_cols.p, nc, W.p);
             k_aux_first<<<blocks_for(rows), 256, 0, s->stream>>>(rows, nc, W.p, tau, d_first.p);
@@ -1819,7 +1821,7 @@ int solve_prepare(spk_system *s) {
     SPK_CUDA(cudaMemcpy(lvl.data(), s->d_lvl.p, sizeof(int) * (P + 1), cudaMemcpyDeviceToHost));
     std::vector<int> keep(std::max(s->rss, 1), 0);
     if (s->rss > 0) {
-        DBuf<int> d_keep;
+        DBuf<int> d_keep(s->stream);
         SPK_TRY(d_keep.alloc(s->rss));
         k_reduced_keep<<<blocks_for(s->rss), 256, 0, s->stream>>>(s->rss, s->IT.p, s->T.p,
                                                                  tau >= 0 ? tau : -1.0, d_keep.p);
@@ -1850,7 +1852,7 @@ int solve_prepare(spk_system *s) {
     SPK_CUDA(cudaGetLastError());
     // sliced ELL of the off-diagonals; kept when padding stays within 2x the off-diagonals
     {
-        DBuf<int> width;
+        DBuf<int> width(s->stream);
         SPK_TRY(width.alloc(ntiles + 1));
         SPK_CUDA(cudaMemsetAsync(width.p, 0, sizeof(int) * (ntiles + 1), s->stream));
         k_ell_width<<<blocks_for(32ll * ntiles), 256, 0, s->stream>>>(s->n, s->uia.p, width.p);
@@ -2116,6 +2118,9 @@ int scaled_residual(spk_system *s, int K, cudaStream_t st, double *out) {
 
 }  // namespace
 
+// diag and ||A|| for the residuals (read from the CSR, which spk_compact releases)
+int residual_prepare(spk_system *s) { return ensure_residual(s); }
+
 int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph) {
     if (!s->built) {
         set_error(SPK_ERR_STATE, "no preprocessed system");
@@ -2137,7 +2142,7 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         if (s->ev_pending[ring]) SPK_TRY(collect_event_set(s, ring));
         cudaEventRecord(s->ev[ring][0], st);
     }
-    if (s->chain_ok && !ph) {
+    if (s->chain_ok && (!ph || s->lean)) {  // a compacted system has no other path (no phase times)
         SPK_TRY(chain_solve(s, b, x, st, prof, ring));
     } else if (s->ell_ok && !ph) {
         SPK_TRY((launch_tiles<1, double>(s, b, s->n, x, s->n, s->xbuf.p, st, prof, ring)));
@@ -2287,7 +2292,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     // count measured); FP32 + refinement: the chain kernel when the partitions give
     // too few tasks to fill the GPU
     const char *cb = getenv("SPK_CHAIN_BATCH");  // 1: always the chain kernels, 0: never
-    const bool use_chain = s->chain_ok && (cb ? cb[0] == '1' : (mode == 0 || !part_wide));
+    const bool use_chain = s->chain_ok && (s->lean || (cb ? cb[0] == '1' : (mode == 0 || !part_wide)));
     if (use_chain) {
         // the chain tasks fill the GPU whatever the partition count: every group
         // of up to 32 columns is one right-hand-side-parallel chain solve (used
@@ -2440,6 +2445,10 @@ int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, 
                        cudaStream_t st) {
     if (!s->built) {
         set_error(SPK_ERR_STATE, "no preprocessed system");
+        return SPK_ERR_STATE;
+    }
+    if (s->lean) {
+        set_error(SPK_ERR_STATE, "the system was compacted (spk_compact): the static batched solve needs its partition pools");
         return SPK_ERR_STATE;
     }
     const long long n = s->n;
@@ -2780,6 +2789,10 @@ int spk_group_create(spk_group **out, int count, spk_system *const *systems, con
             set_error(SPK_ERR_ARG, "group member %d: needs a preprocessed system on the sliced-ELL layout, nrhs > 0 "
                                    "and leading dimensions >= n", i);
             return fail(SPK_ERR_ARG);
+        }
+        if (s->lean) {
+            set_error(SPK_ERR_STATE, "group member %d was compacted (spk_compact): groups need the partition pools", i);
+            return fail(SPK_ERR_STATE);
         }
         if (mode == 1) {
             int rc = ensure_fp32(s);

@@ -50,19 +50,30 @@ template <typename T>
 struct DBuf {
     T *p = nullptr;
     size_t n = 0;
+    // A scoped temporary used only on one stream is allocated and freed in that
+    // stream's order (cudaMallocAsync / cudaFreeAsync): its release does not
+    // wait for the whole device, as cudaFree does, while other threads' solves
+    // run.  Host copies into it go through that stream.
+    cudaStream_t ord = nullptr;
+    bool on_stream = false;
     DBuf() = default;
+    explicit DBuf(cudaStream_t s) : ord(s), on_stream(true) {}
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (on_stream) cudaFreeAsync(p, ord);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
     }
     int alloc(size_t count) {
         release();
         if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        cudaError_t e = on_stream ? cudaMallocAsync((void **)&p, count * sizeof(T), ord)
+                                  : cudaMalloc((void **)&p, count * sizeof(T));
         if (e != cudaSuccess) {
             p = nullptr;
             set_error(SPK_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
@@ -190,6 +201,7 @@ struct spk_system {
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     int dbg_fail_waits = 0;  // test hook: solve kernels report a failed wait at entry (spk_debug_set)
+    int lean = 0;  // spk_compact: only what the chain solves read is kept (partition paths refused)
     // optional per-phase device timing (spk_set_profiling)
     int profiling = 0;
     static constexpr int kEvRing = 64;           // event sets in flight before a forced collection
@@ -213,6 +225,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
 int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, double *X, long long ldx,
                        cudaStream_t st);
 int solve_prepare(spk_system *s);
+int residual_prepare(spk_system *s);
 int chain_prepare(spk_system *s);
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);

@@ -19,7 +19,7 @@ MODE_FP64 = 0
 MODE_FP32_IR = 1
 STATS = ("resident_bytes", "staging_bytes", "resident_systems", "evictions", "preprocessings", "batches",
          "rhs_batched", "completed", "budget", "nomem_retries", "rechecks", "us_stage_in", "us_solve",
-         "us_stage_out", "us_preprocess")
+         "us_stage_out", "us_preprocess", "compactions")
 
 _bound = False
 

@@ -77,10 +77,45 @@ def test_results_are_the_same_alone_and_in_the_mix(mode):
     assert st["preprocessings"] == len(mats)
 
 
+def _footprints(mats, P=8):
+    """Device bytes of each matrix's system, whole and compacted (spk_compact)."""
+    from spike_pstrsv_b200.capi import System
+
+    full, lean = [], []
+    for L in mats:
+        S = System().preproc(L.a, L.ia, L.ja, L.m, P, "L", 1)
+        full.append(S.scalar("device_bytes"))
+        S.compact()
+        lean.append(S.scalar("device_bytes"))
+        S.close()
+    return full, lean
+
+
+def test_idle_systems_are_compacted_before_any_eviction():
+    mats = _pool(count=4, seed=5)
+    full, lean = _footprints(mats)
+    # every system fits once compacted, not all of them whole
+    budget = sum(lean) + (sum(full) - sum(lean)) // 2 + (48 << 20)
+    with serve.Server(hbm_budget_bytes=budget, slots=1) as S:
+        for i, L in enumerate(mats):
+            S.put_matrix(i, L.a, L.ia, L.ja, L.m, 8, "L")
+        for rnd in range(2):
+            for i, L in enumerate(mats):
+                Xt, B = synth.make_rhs(L, seed=11 * i + rnd, nrhs=4)
+                for mode in (serve.MODE_FP32_IR, serve.MODE_FP64):
+                    r = S.submit(i, B, mode).wait()
+                    assert r.scaled_residual <= TOL
+                    assert _rel(r.x, Xt) <= 1e-11
+        st = S.stats()
+    assert st["compactions"] > 0
+    assert st["resident_bytes"] <= budget
+
+
 def test_lru_eviction_under_a_small_budget():
     mats = _pool(count=4, seed=3)
-    # room for about two resident systems with their batch buffers
-    with serve.Server(hbm_budget_bytes=150 << 20, slots=2) as S:
+    full, lean = _footprints(mats)
+    # room for about two resident systems, even compacted, with their batch buffers
+    with serve.Server(hbm_budget_bytes=sum(lean) // 2 + (24 << 20), slots=2) as S:
         for i, L in enumerate(mats):
             S.put_matrix(i, L.a, L.ia, L.ja, L.m, 8, "L")
         for rnd in range(2):
