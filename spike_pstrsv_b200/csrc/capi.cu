@@ -132,6 +132,7 @@ void destroy_system(spk_system *s) {
         for (auto &e : set)
             if (e) cudaEventDestroy(e);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    if (s->pipe_exec) cudaGraphExecDestroy(s->pipe_exec);
     for (cudaEvent_t e : s->pipe_ev) cudaEventDestroy(e);
     for (cudaStream_t q : s->pipe_st) cudaStreamDestroy(q);
     if (s->st_in) cudaStreamDestroy(s->st_in);

@@ -1010,6 +1010,11 @@ void chain_release(spk_system *s) {
     s->cp_batch.release();
     s->cp_host.release();
     s->host_plan_tried = 0;
+    if (s->pipe_exec) cudaGraphExecDestroy(s->pipe_exec);
+    s->pipe_exec = nullptr;
+    s->pipe_b = s->pipe_db = nullptr;
+    s->pipe_x = s->pipe_dx = nullptr;
+    s->pipe_K = 0;
     s->h_ctasks1.clear();
     s->h_ctasks4.clear();
     s->nctasks1 = s->nctasks4 = 0;
@@ -1201,6 +1206,8 @@ int chain_rhs_occupancy(spk_system *s, int *occ) {
 // chain below); its x is copied out on s->st_out once its phase 4 is done.  One
 // cudaMemcpyAsync per chunk and direction; overlap needs page-locked b and x
 // (pageable memory gives the same result with the copies serialised).
+int chain_pipeline(spk_system *s, const double *b, double *x, double *db, double *dx, int K);
+
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx) {
     // After the last copy lands, one chain still has to be solved before its rows
     // can leave: the pipeline takes chains of at most 2,048 rows (built once,
@@ -1211,11 +1218,7 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
         if (const char *e = getenv("SPK_PIPELINE_ROWS")) len = std::max(32ll, 32ll * ((atoll(e) + 31) / 32));
         if (len < s->ch_len) SPK_TRY(build_plan(s, len, s->ch_reach, &s->cp_host));
     }
-    const ChainPlan &hp = s->cp_host;
-    const bool own = hp.len > 0;
-    const std::vector<ChainTask> &T1 = own ? hp.h1 : s->h_ctasks1, &T4 = own ? hp.h4 : s->h_ctasks4;
-    const ChainTask *D1 = own ? hp.d1.p : s->d_ctasks1.p, *D4 = own ? hp.d4.p : s->d_ctasks4.p;
-    const int n = s->n, nch = (int)T1.size(), n4 = (int)T4.size();
+    const int nch = (int)(s->cp_host.len > 0 ? s->cp_host.h1.size() : s->h_ctasks1.size());
     int K = 16;
     if (const char *e = getenv("SPK_PIPELINE_CHUNKS")) K = std::max(1, atoi(e));
     K = std::min(K, std::max(nch, 1));
@@ -1233,6 +1236,64 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
         SPK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         s->pipe_ev.push_back(e);
     }
+    // the same page-locked b and x (and device copies, chunk count) as the last
+    // call: replay the pipeline captured then; the second such call captures it
+    const bool same = s->pipe_b == b && s->pipe_x == x && s->pipe_db == db && s->pipe_dx == dx && s->pipe_K == K;
+    if (same && s->pipe_exec) {
+        SPK_CUDA(cudaGraphLaunch(s->pipe_exec, s->stream));
+        SPK_CUDA(cudaStreamSynchronize(s->stream));
+        return SPK_OK;
+    }
+    if (!same) {
+        if (s->pipe_exec) cudaGraphExecDestroy(s->pipe_exec);
+        s->pipe_exec = nullptr;
+        s->pipe_b = b;
+        s->pipe_x = x;
+        s->pipe_db = db;
+        s->pipe_dx = dx;
+        s->pipe_K = K;
+    }
+    auto locked = [](const void *p) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    const bool capture = same && !s->pipe_nograph && locked(b) && locked(x);
+    if (capture) SPK_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = chain_pipeline(s, b, x, db, dx, K);
+    if (capture) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        cudaGraphExec_t ex = nullptr;
+        if (rc == SPK_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (rc != SPK_OK) return rc;
+        if (e == cudaSuccess) {
+            s->pipe_exec = ex;
+            SPK_CUDA(cudaGraphLaunch(ex, s->stream));
+        } else {
+            cudaGetLastError();
+            s->pipe_nograph = 1;  // not capturable here: the direct pipeline from now on
+            SPK_TRY(chain_pipeline(s, b, x, db, dx, K));
+        }
+    } else {
+        SPK_TRY(rc);
+    }
+    SPK_CUDA(cudaStreamSynchronize(s->stream));
+    return SPK_OK;
+}
+
+// The pipeline's copies and launches, forked from and joined back to the
+// system's stream (nothing here synchronizes: it may be captured).
+int chain_pipeline(spk_system *s, const double *b, double *x, double *db, double *dx, int K) {
+    const ChainPlan &hp = s->cp_host;
+    const bool own = hp.len > 0;
+    const std::vector<ChainTask> &T1 = own ? hp.h1 : s->h_ctasks1, &T4 = own ? hp.h4 : s->h_ctasks4;
+    const ChainTask *D1 = own ? hp.d1.p : s->d_ctasks1.p, *D4 = own ? hp.d4.p : s->d_ctasks4.p;
+    const int n = s->n, nch = (int)T1.size(), n4 = (int)T4.size();
     cudaEvent_t *ev_in = s->pipe_ev.data(), *ev_p1 = ev_in + K, *ev_done = ev_in + 2 * K, *ev_start = ev_in + 3 * K;
     const bool rev = s->uplo == 'L';
     // chunk k: chains [c0(k), c0(k+1)), U rows [A(k), Q(k)), phase-4 tasks [t0(k), t0(k+1))
@@ -1262,26 +1323,32 @@ int chain_solve_host(spk_system *s, const double *b, double *x, double *db, doub
         SPK_CUDA(cudaMemcpyAsync(db + lo, b + lo, sizeof(double) * cnt, cudaMemcpyHostToDevice, s->st_in));
         SPK_CUDA(cudaEventRecord(ev_in[k], s->st_in));
     }
-    for (int k = 0; k < K; k++) {
-        cudaStream_t q = s->pipe_st[k];
-        SPK_CUDA(cudaStreamWaitEvent(q, ev_in[k], 0));
-        SPK_TRY(launch_chain<false>(s, D1 + c0[k], c0[k + 1] - c0[k], db, dx, q));
-        SPK_CUDA(cudaEventRecord(ev_p1[k], q));
-    }
-    for (int k = 0; k < K; k++) {
-        cudaStream_t q = s->pipe_st[k];
-        if (k + 1 < K) SPK_CUDA(cudaStreamWaitEvent(q, ev_p1[k + 1], 0));
-        SPK_TRY(launch_chain<true>(s, D4 + t0[k], t0[k + 1] - t0[k], db, dx, q));
-        SPK_CUDA(cudaEventRecord(ev_done[k], q));
-        int lo, cnt;
-        lo_rows(k, lo, cnt);
-        SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_done[k], 0));
-        SPK_CUDA(cudaMemcpyAsync(x + lo, dx + lo, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s->st_out));
+    // chunk k's phase 1 on stream k; phase 4 of chunk k-1 (which reads the first
+    // rows of chunk k) right behind it on the same stream: streams share the
+    // device's hardware queues, and a launch queued behind one it does not
+    // depend on would wait for it
+    for (int k = 0; k <= K; k++) {
+        if (k < K) {
+            cudaStream_t q = s->pipe_st[k];
+            SPK_CUDA(cudaStreamWaitEvent(q, ev_in[k], 0));
+            SPK_TRY(launch_chain<false>(s, D1 + c0[k], c0[k + 1] - c0[k], db, dx, q));
+            SPK_CUDA(cudaEventRecord(ev_p1[k], q));
+        }
+        if (k > 0) {
+            const int j = k - 1;
+            cudaStream_t q = s->pipe_st[k < K ? k : K - 1];
+            if (k < K) SPK_CUDA(cudaStreamWaitEvent(q, ev_p1[j], 0));
+            SPK_TRY(launch_chain<true>(s, D4 + t0[j], t0[j + 1] - t0[j], db, dx, q));
+            SPK_CUDA(cudaEventRecord(ev_done[j], q));
+            int lo, cnt;
+            lo_rows(j, lo, cnt);
+            SPK_CUDA(cudaStreamWaitEvent(s->st_out, ev_done[j], 0));
+            SPK_CUDA(cudaMemcpyAsync(x + lo, dx + lo, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s->st_out));
+        }
     }
     // the system's stream continues after the whole solve
     SPK_CUDA(cudaEventRecord(ev_start[0], s->st_out));
     SPK_CUDA(cudaStreamWaitEvent(s->stream, ev_start[0], 0));
-    SPK_CUDA(cudaStreamSynchronize(s->st_out));
     return SPK_OK;
 }
 

@@ -198,6 +198,12 @@ struct spk_system {
     cudaStream_t st_in = nullptr, st_out = nullptr;  // copy streams of the pipelined host-array solve
     std::vector<cudaEvent_t> pipe_ev;
     std::vector<cudaStream_t> pipe_st;  // one per chunk of the pipelined solve
+    // the pipeline captured as a graph, replayed while the caller keeps the same
+    // page-locked b and x (and the same device copies and chunk count)
+    cudaGraphExec_t pipe_exec = nullptr;
+    const double *pipe_b = nullptr, *pipe_db = nullptr;
+    double *pipe_x = nullptr, *pipe_dx = nullptr;
+    int pipe_K = 0, pipe_nograph = 0;
     spk::DBuf<int> d_red_rows, d_red_off, d_err;  // kept reduced rows by level; device error flag
     int nlvl = 0, nkept = 0;
     int dbg_fail_waits = 0;  // test hook: solve kernels report a failed wait at entry (spk_debug_set)
