@@ -16,6 +16,7 @@ import argparse
 import ctypes
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -121,6 +122,22 @@ def autotune(mats, nrhs, mode: int = MODE_FP64, candidates=ROWS_PER_PARTITION, r
         classes.setdefault(size_class(L.m), []).append(i)
     choice, table = {}, {}
     stream = torch.cuda.current_stream()
+    # the group runs the partition kernels, whose speed the partition count sets;
+    # a single system's batched solve would take the chain kernels, which do not
+    # depend on it, so the timings force the partition path
+    saved = os.environ.get("SPK_CHAIN_BATCH")
+    os.environ["SPK_CHAIN_BATCH"] = "0"
+    try:
+        return _autotune_classes(mats, nrhs, mode, candidates, reps, classes, choice, table, stream)
+    finally:
+        if saved is None:
+            os.environ.pop("SPK_CHAIN_BATCH", None)
+        else:
+            os.environ["SPK_CHAIN_BATCH"] = saved
+
+
+def _autotune_classes(mats, nrhs, mode, candidates, reps, classes, choice, table, stream):
+    import torch
     for c, idx in sorted(classes.items()):
         idx = sorted(idx, key=lambda i: mats[i].m)
         rep = idx[len(idx) // 2]
