@@ -175,7 +175,8 @@ void spk_mtx_free(double *a, int *ia, int *ja);
 
 /* Lend the system device memory for the batched solves' work columns (no
  * reference counterpart): with a workspace set, spk_solve_batch carves its
- * work, residual and correction columns (32 x n FP64 each, as needed) from it
+ * work, residual and correction columns (32 x n FP64 each, as needed; FP32 +
+ * refinement adds 32 FP64 columns of the reduced system's unknowns) from it
  * instead of buffers it allocates and keeps with the system, and the system's
  * own batch buffers are released.  spk_workspace_bytes gives the size a mode
  * needs (mode SPK_MODE_FP64 or SPK_MODE_FP32_IR; with_residual: FP64 batches

@@ -479,7 +479,9 @@ int spk_set_workspace(spk_system *s, void *dev_ptr, long long bytes) {
 long long spk_workspace_bytes(const spk_system *s, int mode, int with_residual) {
     if (!s) return -1;
     const long long col = ((32ll * s->n * 8) + 255) / 256 * 256;
-    return col * (1 + (mode == 1 || with_residual) + (mode == 1));
+    // FP32 + refinement also keeps the reduced unknowns in FP64 (32 columns)
+    const long long red = mode == 1 ? 32ll * s->nRed * 8 : 0;
+    return col * (1 + (mode == 1 || with_residual) + (mode == 1)) + red;
 }
 
 int spk_set_profiling(spk_system *s, int on) {

@@ -1210,7 +1210,10 @@ __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || 
 // ---- batched solve support --------------------------------------------------------
 
 // Reduced solve on the kept rows for K right-hand sides stored in T with FP64
-// accumulation (same level structure as k_reduced_solve).
+// accumulation (same level structure as k_reduced_solve).  With FP32 storage and
+// an FP64 scratch `red` ([K][nred]), the reduced unknowns are gathered into it,
+// every level is solved and stored in FP64, and they are rounded to T once, on
+// the way back: the coupled boundary system stays FP64 throughout.
 template <int K>
 constexpr int red_threads() { return K >= 16 ? 512 : 1024; }  // K >= 16: registers for the K sums
 
@@ -1218,8 +1221,43 @@ template <int K, typename T>
 __device__ __forceinline__ void reduced_body(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
                                              const int *__restrict__ mapRedX, const int *__restrict__ IT,
                                              const int *__restrict__ JT, const double *__restrict__ Tv,
-                                             T *__restrict__ xbuf, int n) {
+                                             T *__restrict__ xbuf, int n, double *__restrict__ red, int nred) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    if (red) {
+        for (long long e = threadIdx.x; e < (long long)K * nred; e += blockDim.x) {
+            const int k = (int)(e / nred), i = (int)(e % nred);
+            red[e] = (double)xbuf[(long long)k * n + mapRedX[i]];
+        }
+        __syncthreads();
+        for (int li = 0; li < nlvl; li++) {
+            for (int q = lvl_off[li] + warp; q < lvl_off[li + 1]; q += nwarps) {
+                const int kr = rows[q];
+                double sum[K];
+#pragma unroll
+                for (int k = 0; k < K; k++) sum[k] = 0.0;
+                for (int j = IT[kr] + lane; j < IT[kr + 1]; j += 32) {
+                    const int c = JT[j];
+#pragma unroll
+                    for (int k = 0; k < K; k++) sum[k] = fma(Tv[j], red[(long long)k * nred + c], sum[k]);
+                }
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+#pragma unroll
+                    for (int o = 16; o; o >>= 1) sum[k] += __shfl_xor_sync(0xffffffffu, sum[k], o);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int k = 0; k < K; k++) red[(long long)k * nred + kr] -= sum[k];
+                }
+            }
+            __syncthreads();
+        }
+        for (long long e = threadIdx.x; e < (long long)K * nred; e += blockDim.x) {
+            const int k = (int)(e / nred), i = (int)(e % nred);
+            xbuf[(long long)k * n + mapRedX[i]] = (T)red[e];
+        }
+        return;
+    }
     for (int li = 0; li < nlvl; li++) {
         for (int q = lvl_off[li] + warp; q < lvl_off[li + 1]; q += nwarps) {
             const int kr = rows[q];
@@ -1250,8 +1288,8 @@ template <int K, typename T>
 __global__ void __launch_bounds__(red_threads<K>())
 k_reduced_solve_k(const int *__restrict__ rows, const int *__restrict__ lvl_off, int nlvl,
                   const int *__restrict__ mapRedX, const int *__restrict__ IT, const int *__restrict__ JT,
-                  const double *__restrict__ Tv, T *__restrict__ xbuf, int n) {
-    reduced_body<K, T>(rows, lvl_off, nlvl, mapRedX, IT, JT, Tv, xbuf, n);
+                  const double *__restrict__ Tv, T *__restrict__ xbuf, int n, double *__restrict__ red, int nred) {
+    reduced_body<K, T>(rows, lvl_off, nlvl, mapRedX, IT, JT, Tv, xbuf, n, red, nred);
 }
 
 // Reduced solves of many systems: block b takes the system of args[list[b]].
@@ -1262,12 +1300,14 @@ struct RedArgs {
     const double *Tv;
     void *xbuf;  // T
     int n;
+    double *red;  // FP64 reduced unknowns of an FP32 batch ([K][nred]), or null
+    int nred;
 };
 
 template <int K, typename T>
 __global__ void __launch_bounds__(red_threads<K>()) k_reduced_multi(const RedArgs *__restrict__ args) {
     const RedArgs A = args[blockIdx.x];
-    reduced_body<K, T>(A.rows, A.lvl_off, A.nlvl, A.mapRedX, A.IT, A.JT, A.Tv, (T *)A.xbuf, A.n);
+    reduced_body<K, T>(A.rows, A.lvl_off, A.nlvl, A.mapRedX, A.IT, A.JT, A.Tv, (T *)A.xbuf, A.n, A.red, A.nred);
 }
 
 // R = B - A X in FP64 on the ELL copy (plus the diagonal), in the caller's order
@@ -1924,7 +1964,8 @@ int launch_tiles(spk_system *s, const double *rhs, long long ldb, double *xo, lo
     if (prof) cudaEventRecord(s->ev[ring][1], st);
     if (s->redNec && s->nkept) {
         k_reduced_solve_k<K, T><<<1, red_threads<K>(), 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
-                                                     s->IT.p, s->JT.p, s->T.p, work, s->n);
+                                                     s->IT.p, s->JT.p, s->T.p, work, s->n,
+                                                     sizeof(T) == 4 ? s->red_scratch : nullptr, s->nRed);
         SPK_CUDA(cudaGetLastError());
         s->launches++;
     }
@@ -1982,7 +2023,8 @@ int launch_rhs(spk_system *s, int nk, const double *rhs, long long ldb, double *
     }
     if (s->redNec && s->nkept) {
         k_reduced_solve_k<32, T><<<1, red_threads<32>(), 0, st>>>(s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p,
-                                                      s->IT.p, s->JT.p, s->T.p, work, s->n);
+                                                      s->IT.p, s->JT.p, s->T.p, work, s->n,
+                                                      sizeof(T) == 4 ? s->red_scratch : nullptr, s->nRed);
         SPK_CUDA(cudaGetLastError());
         s->launches++;
     }
@@ -2255,8 +2297,10 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
         SPK_TRY(ensure_reach(s));
     }
     if (need_r) SPK_TRY(ensure_residual(s));
+    // FP32 batches: the FP64 reduced unknowns (32 columns), after the other blocks
+    const size_t red_bytes = mode == 1 ? (size_t)32 * s->nRed * sizeof(double) : 0;
     if (s->ext_ws) {
-        const size_t need = col_bytes * (1 + need_r + need_d);
+        const size_t need = col_bytes * (1 + need_r + need_d) + red_bytes;
         if (s->ext_ws_bytes < need) {
             set_error(SPK_ERR_TOO_LARGE, "workspace of %zu bytes is below the %zu this batch needs", s->ext_ws_bytes,
                       need);
@@ -2359,8 +2403,19 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
                 worst = worst_of(worst, r);
             }
         } else {
-            SPK_TRY(work_for(sizeof(float) * wcols * n));
+            // FP32 work columns, then the FP64 reduced unknowns (a lent
+            // workspace holds them after its column blocks)
+            const size_t fbytes = (sizeof(float) * wcols * n + 255) / 256 * 256;
+            const bool red64 = s->redNec && s->nkept;
+            SPK_TRY(work_for(fbytes + (red64 ? red_bytes : 0)));
             float *wk = (float *)work_p;
+            s->red_scratch = !red64 ? nullptr
+                             : s->ext_ws ? (double *)(s->ext_ws + col_bytes * (1 + need_r + need_d))
+                                         : (double *)(work_p + fbytes);
+            struct ClearRed {
+                spk_system *s;
+                ~ClearRed() { s->red_scratch = nullptr; }
+            } clear_red{s};
             auto solve32 = [&](const double *rhs, long long ld, double *xo, long long ldo) {
                 return rhs_path ? launch_rhs<float>(s, K, rhs, ld, xo, ldo, wk, st)
                                : launch_tiles_k<float>(s, K, rhs, ld, xo, ldo, wk, st);
@@ -2560,6 +2615,7 @@ struct GroupVS {
     long long ldx;
     char *work;
     double *R, *D;
+    double *red;  // FP32 batches: the FP64 reduced unknowns ([K][nRed])
 };
 
 struct GroupClass {
@@ -2656,7 +2712,7 @@ int build_class(spk_group *g, GroupClass &c, const std::vector<std::vector<SegTa
         }
         if (s->redNec && s->nkept) {
             RedArgs r{s->d_red_rows.p, s->d_red_off.p, s->nlvl, s->mapRedX.p, s->IT.p, s->JT.p, s->T.p, v.work,
-                      s->n};
+                      s->n, fp32 ? v.red : nullptr, s->nRed};
             red.push_back(r);
             cred.push_back(r);
         }
@@ -2833,6 +2889,8 @@ int spk_group_create(spk_group **out, int count, spk_system *const *systems, con
                 pool_bytes += (kn * 8 + 255) / 256 * 256;
                 v.D = (double *)(intptr_t)pool_bytes;
                 pool_bytes += (kn * 8 + 255) / 256 * 256;
+                v.red = (double *)(intptr_t)pool_bytes;
+                pool_bytes += ((long long)K * s->nRed * 8 + 255) / 256 * 256;
             }
             g->vs.push_back(v);
             cols += K;
@@ -2848,6 +2906,7 @@ int spk_group_create(spk_group **out, int count, spk_system *const *systems, con
         if (mode == 1) {
             v.R = (double *)(g->pool.p + (intptr_t)v.R);
             v.D = (double *)(g->pool.p + (intptr_t)v.D);
+            v.red = (double *)(g->pool.p + (intptr_t)v.red);
         }
     }
     for (int c = 0; c < 5; c++) g->cls[c].K = kGroupK[c];

@@ -208,6 +208,7 @@ struct spk_system {
     int nlvl = 0, nkept = 0;
     int dbg_fail_waits = 0;  // test hook: solve kernels report a failed wait at entry (spk_debug_set)
     int lean = 0;  // spk_compact: only what the chain solves read is kept (partition paths refused)
+    double *red_scratch = nullptr;  // FP64 reduced unknowns of the FP32 batched solve in flight
     // optional per-phase device timing (spk_set_profiling)
     int profiling = 0;
     static constexpr int kEvRing = 64;           // event sets in flight before a forced collection
