@@ -72,7 +72,8 @@ void logPSTRSV3(int nthreads);
 /* Flags with the reference's names and defaults (src/spike_pstrsv_ops.c:63-65). */
 extern char PSTRSV_VERBOSE;        /* 1: logPSTRSV3 after preprocessing */
 extern char FORCE_LOAD_BALANCE;    /* 1 (default): optimizeLoadBalance step */
-extern char IS_MATRIX_PARTITIONED; /* 1: use partition_starts/ends as set by the caller, then reset */
+extern char IS_MATRIX_PARTITIONED; /* 1: use partition_starts/ends as set by the caller (rows of the
+                                      caller's matrix, also for 'L'), then reset */
 extern char SPK_CLOBBER_B;         /* 1: write the corrected right-hand side back into b */
 extern char SPK_EXACT;             /* 1: no spike truncation (see spk_set_truncation) */
 
@@ -132,7 +133,10 @@ int spk_destroy(spk_system *s);
 
 /* Preprocess (a, ia, ja) into nparts partitions.  Host or device pointers.
  * flb: FORCE_LOAD_BALANCE.  starts/ends: optional host arrays of nparts
- * contiguous partition bounds (the IS_MATRIX_PARTITIONED path), else NULL. */
+ * contiguous partition bounds (the IS_MATRIX_PARTITIONED path), else NULL, in
+ * the caller's row order: for uplo 'L', partition t (rows [starts[t], ends[t])
+ * of L) is partition nparts-1-t of the mirror J L J, which the structure
+ * arrays describe. */
 int spk_preproc(spk_system *s, const double *a, const int *ia, const int *ja, int n, int nparts,
                 char uplo, int flb, const int *starts, const int *ends);
 
@@ -172,6 +176,47 @@ void matrixMarketToCSR(const char *filename, double **a, MKL_INT **ia, MKL_INT *
  * files) and the entry count. */
 int spk_mtx_read(const char *path, char uplo, char symm, double **a, int **ia, int **ja, int *n, int *nnz);
 void spk_mtx_free(double *a, int *ia, int *ja);
+
+/* Replace pathToMatrixName and strconcat (src/misc.h, src/misc.c:254-297), which
+ * the reference's profiler calls: base name of a path without its extension,
+ * and the concatenation of two strings, both malloc'd (free()). */
+char *pathToMatrixName(const char *filepath);
+char *strconcat(const char *str1, const char *str2);
+
+/* Partition-aware reordering (src/matrix_reordering.h:16-41,
+ * src/matrix_reordering.c:18-356), host CSR arrays from malloc/posix_memalign
+ * (matrixMarketToCSR's), freed and replaced where a function returns a new
+ * matrix.
+ * matrixReordering: (*a, *ia, *ja) is the full n x n matrix.  Unless the
+ * nthreads equal partitions already decouple (matrixAnalysis), the rows are
+ * renumbered for nthreads partitions and the matrix becomes the upper (uplo
+ * 'U') or lower (otherwise) triangle of the renumbered matrix, with
+ * partition_starts/ends/numRows set and IS_MATRIX_PARTITIONED = 1 for the next
+ * spike_pstrsv_preproc.  The partitioner replaces the reference's METIS k-way
+ * call: a reverse Cuthill-McKee order of the pattern of A + A^T cut into
+ * nthreads contiguous ranges of nearly equal nonzero count; rows are then
+ * grouped by partition in their original order, as in the reference.  The
+ * renumbering and triangle run on the GPU.
+ * matrixAnalysis: 1 (and the matrix replaced by its triangle, re-read from
+ * matrixFileName, or taken in memory when it is NULL) when no entry of the
+ * triangle couples two equal partitions, else 0.
+ * matrixSymmetrization: A <- A + A^T, values summed, sorted columns.
+ * matrixDuplication: copies of the three arrays. */
+void matrixReordering(double **a, MKL_INT **ia, MKL_INT **ja, int numRows, int nthreads, const char uplo,
+                      const char symm, const char *matrixFileName);
+int matrixAnalysis(int numRows, int nthreads, double **a, MKL_INT **ia, MKL_INT **ja, const char uplo,
+                   const char symm, const char *matrixFileName);
+void matrixSymmetrization(double **a, MKL_INT **ia, MKL_INT **ja, int numRows);
+void matrixDuplication(int numRows, double *a, MKL_INT *ia, MKL_INT *ja, double **a_dup, MKL_INT **ia_dup,
+                       MKL_INT **ja_dup);
+/* Status-returning reordering (no reference counterpart): matrixReordering's
+ * renumbering and triangle without the matrixAnalysis shortcut; perm (optional,
+ * n ints) receives the original row of every new row. */
+int spk_reorder(double **a, int **ia, int **ja, int n, int nparts, char uplo, int *perm);
+/* The reordering's partitioner alone, host code (no GPU): order[q] = the row at
+ * position q of the reverse Cuthill-McKee order, part[r] = the partition of row
+ * r (both optional, n ints). */
+int spk_reorder_plan(int n, const int *ia, const int *ja, int nparts, int *order, int *part);
 
 /* Lend the system device memory for the batched solves' work columns (no
  * reference counterpart): with a workspace set, spk_solve_batch carves its

@@ -21,6 +21,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspike_ref.so")
+# The reference's own drivers built against the GPU library (Makefile target
+# ``drivers``); they exercise the product, the tests only run them.
+PROFILER_BIN = os.path.join(HERE, "_ref", "runtimeAnalysis")
+EXAMPLE_BIN = os.path.join(HERE, "_ref", "exampleUsage")
 
 _DT = {"d": np.float64, "i": np.int32, "q": np.int64, "c": np.int8}
 _CT = {"d": ctypes.c_double, "i": ctypes.c_int32, "q": ctypes.c_int64, "c": ctypes.c_int8}
@@ -47,6 +51,9 @@ def build(ref: bool | None = None) -> None:
         ref = os.path.isdir(src)
     if ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref", "SPK_REF_SRC=" + src], check=True)
+        # the reference's profiler and example, linked against the GPU library
+        # (built before this by __graft_entry__.build)
+        subprocess.run(["make", "-s", "-C", HERE, "drivers", "SPK_REF_SRC=" + src], check=True)
 
 
 def ref_source_dir() -> str:
@@ -209,6 +216,49 @@ class Reference:
         f = self.lib()._spike_pstrsv_solve if timed else self.lib().spike_pstrsv_solve
         f(b"U", self.m, bb.ctypes.data + 8 * pad, xx.ctypes.data + 8 * pad, self.P)
         return xx[pad:pad + self.m].copy()
+
+    def set_partitions(self, starts, ends) -> None:
+        """Caller-set partition bounds for the next preproc (IS_MATRIX_PARTITIONED,
+        src/matrix_partitioning.c:23-35; the solve reads partition_numRows too)."""
+        I = ctypes.c_int32
+        for name, vals in (("partition_starts", starts), ("partition_ends", ends),
+                           ("partition_numRows", np.asarray(ends) - np.asarray(starts))):
+            base = ctypes.addressof(self._sym(name, I))
+            for k, v in enumerate(vals):
+                I.from_address(base + 4 * k).value = int(v)
+        self.set_flag("IS_MATRIX_PARTITIONED", 1)
+
+    def reorder(self, A, P: int, uplo: str, part) -> tuple:
+        """The reference's matrixReordering (src/matrix_reordering.c:83-305) on the
+        full matrix A (symmetric pattern, symm 'Y'), with its METIS call answered
+        by `part` (ref/reorder_stubs.c).  Returns (a, ia, ja, starts, ends,
+        numRows) and leaves IS_MATRIX_PARTITIONED set for the next preproc."""
+        lib = self.lib()
+        lib.mkl_malloc.restype = ctypes.c_void_p
+        lib.mkl_malloc.argtypes = [ctypes.c_size_t, ctypes.c_int]
+        lib.spk_ref_set_partition.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.matrixReordering.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_char, ctypes.c_char, ctypes.c_char_p]
+        n = int(A.m)
+        pv = _i32(part)
+        lib.spk_ref_set_partition(pv.ctypes.data, n)
+        ptrs = []
+        for arr, ct in ((_f64(A.a), ctypes.c_double), (_i32(A.ia), ctypes.c_int32), (_i32(A.ja), ctypes.c_int32)):
+            p = lib.mkl_malloc(max(arr.nbytes, 8), 64)
+            ctypes.memmove(p, arr.ctypes.data, arr.nbytes)
+            ptrs.append(ctypes.c_void_p(p))
+        lib.matrixReordering(ctypes.byref(ptrs[0]), ctypes.byref(ptrs[1]), ctypes.byref(ptrs[2]), n, int(P),
+                             uplo.encode()[:1], b"Y", None)
+
+        def read(p, ct, count):
+            return np.ctypeslib.as_array((ct * count).from_address(p.value)).copy()
+
+        ia = read(ptrs[1], ctypes.c_int32, n + 1)
+        nnz = int(ia[n])
+        out = (read(ptrs[0], ctypes.c_double, nnz), ia, read(ptrs[2], ctypes.c_int32, nnz))
+        I = ctypes.c_int32
+        bounds = tuple(self._arr(k, I, P) for k in ("partition_starts", "partition_ends", "partition_numRows"))
+        return out + bounds
 
     def solve_raw(self, bbuf_addr: int, xbuf_addr: int, timed: bool = True) -> None:
         f = self.lib()._spike_pstrsv_solve if timed else self.lib().spike_pstrsv_solve

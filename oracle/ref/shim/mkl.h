@@ -19,6 +19,11 @@
  *     published, so parity at this call site is ulp-level, not bitwise.
  *   - mkl_dcsrsm: reachable only from dead code (produceS_PSTRSV3,
  *     produceS_PSTRSV3_Parallel_OLD); it aborts if ever called.
+ *   - mkl_dcsrcoo (matrix_reordering.c:186-187, job = {2, 0, 0, 0, nnz, 0}):
+ *     zero-based coordinate format to zero-based CSR with the column indices
+ *     sorted increasingly within each row.
+ *   - mkl_dcsradd: only reached by matrixSymmetrization for unsymmetric input;
+ *     it aborts if called (the checker runs the reordering on symmetric input).
  */
 #ifndef SPK_MKL_SHIM_H
 #define SPK_MKL_SHIM_H
@@ -43,6 +48,12 @@ void mkl_dcsrsm(const char *transa, const MKL_INT *m, const MKL_INT *n, const do
                 const char *matdescra, const double *val, const MKL_INT *indx,
                 const MKL_INT *pntrb, const MKL_INT *pntre, const double *b,
                 const MKL_INT *ldb, double *c, const MKL_INT *ldc);
+void mkl_dcsrcoo(const MKL_INT *job, const MKL_INT *n, double *acsr, MKL_INT *ja, MKL_INT *ia,
+                 MKL_INT *nnz, double *acoo, MKL_INT *rowind, MKL_INT *colind, MKL_INT *info);
+void mkl_dcsradd(const char *trans, const MKL_INT *request, const MKL_INT *sort, const MKL_INT *m,
+                 const MKL_INT *n, double *a, MKL_INT *ja, MKL_INT *ia, const double *beta, double *b,
+                 MKL_INT *jb, MKL_INT *ib, double *c, MKL_INT *jc, MKL_INT *ic, const MKL_INT *nzmax,
+                 MKL_INT *info);
 
 #ifdef __cplusplus
 }

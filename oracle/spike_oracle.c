@@ -103,15 +103,19 @@ void spko_destroy(spko *s)
     free(s);
 }
 
-/* matrix_partitioning.c:18-36 -- k = n/P rows each, leftovers to the last block. */
+/* matrix_partitioning.c:18-36 -- k = n/P rows each, leftovers to the last block.
+ * Caller bounds (the IS_MATRIX_PARTITIONED path) are in the caller's row order:
+ * for 'L' caller partition t, rows [starts[t], ends[t]) of L, is partition
+ * P-1-t of the mirror J L J, rows [n-ends[t], n-starts[t]). */
 static void partition_rows(spko *s, const int *starts, const int *ends)
 {
     int P = s->P, n = s->n;
     if (starts && ends) {
         for (int t = 0; t < P; t++) {
-            s->ps[t] = starts[t];
-            s->pe[t] = ends[t];
-            s->pnum[t] = ends[t] - starts[t];
+            int c = s->uplo == 'L' ? P - 1 - t : t;
+            s->ps[t] = s->uplo == 'L' ? n - ends[c] : starts[c];
+            s->pe[t] = s->uplo == 'L' ? n - starts[c] : ends[c];
+            s->pnum[t] = s->pe[t] - s->ps[t];
         }
         return;
     }

@@ -18,6 +18,8 @@ from .capi import (  # noqa: F401
     legacy_structure,
     lib,
     logPSTRSV3,
+    reorder,
+    reorder_plan,
     set_flag,
     set_partitions,
     spike_pstrsv,

@@ -349,3 +349,70 @@ def legacy_structure() -> dict:
     out = s.structure()
     s.h = None  # not owned
     return out
+
+
+# ---- partition-aware reordering (src/matrix_reordering.c) --------------------------
+
+def _libc() -> ctypes.CDLL:
+    c = ctypes.CDLL(None)
+    c.malloc.restype = ctypes.c_void_p
+    c.malloc.argtypes = [ctypes.c_size_t]
+    c.free.argtypes = [ctypes.c_void_p]
+    return c
+
+
+def reorder_plan(ia, ja, n: int, nparts: int):
+    """The reordering's partitioner (host code): (order, part), order[q] = the row
+    at position q of the reverse Cuthill-McKee order, part[r] = partition of row r."""
+    L = lib()
+    ia = np.ascontiguousarray(ia, dtype=np.int32)
+    ja = np.ascontiguousarray(ja, dtype=np.int32)
+    order = np.zeros(n, dtype=np.int32)
+    part = np.zeros(n, dtype=np.int32)
+    vp = ctypes.c_void_p
+    L.spk_reorder_plan.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int, vp, vp]
+    _check(L.spk_reorder_plan(int(n), ia.ctypes.data, ja.ctypes.data, int(nparts), order.ctypes.data,
+                              part.ctypes.data))
+    return order, part
+
+
+def reorder(a, ia, ja, n: int, nparts: int, uplo: str = "U", legacy: bool = False):
+    """Reorder the full host CSR (a, ia, ja) for nparts partitions and keep one
+    triangle.  legacy=False: spk_reorder, returns (a, ia, ja, perm).  legacy=True:
+    the reference entry point matrixReordering (symm 'Y', no file), returns
+    (a, ia, ja, None) with the partition globals set and IS_MATRIX_PARTITIONED
+    raised for the next spike_pstrsv_preproc."""
+    L, C = lib(), _libc()
+    arrs = (np.ascontiguousarray(a, dtype=np.float64), np.ascontiguousarray(ia, dtype=np.int32),
+            np.ascontiguousarray(ja, dtype=np.int32))
+    ptrs = []
+    for x in arrs:  # the library frees the inputs with free() and returns malloc'd arrays
+        p = C.malloc(max(x.nbytes, 8))
+        if not p:
+            raise MemoryError("malloc failed")
+        ctypes.memmove(p, x.ctypes.data, x.nbytes)
+        ptrs.append(ctypes.c_void_p(p))
+    refs = [ctypes.byref(p) for p in ptrs]
+    perm = None
+    if legacy:
+        L.matrixReordering.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int, ctypes.c_char,
+                                                               ctypes.c_char, ctypes.c_char_p]
+        L.matrixReordering(*refs, int(n), int(nparts), _uplo(uplo), b"Y", None)
+    else:
+        perm = np.zeros(n, dtype=np.int32)
+        L.spk_reorder.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int, ctypes.c_char,
+                                                          ctypes.c_void_p]
+        rc = L.spk_reorder(*refs, int(n), int(nparts), _uplo(uplo), perm.ctypes.data)
+        if rc != 0:
+            for p in ptrs:
+                C.free(p)
+            _check(rc)
+
+    def take(p, ct, count):
+        out = np.ctypeslib.as_array((ct * max(count, 1)).from_address(p.value))[:count].copy()
+        C.free(p)
+        return out
+
+    ia_o = take(ptrs[1], ctypes.c_int32, n + 1)
+    nnz = int(ia_o[n])
+    return take(ptrs[0], ctypes.c_double, nnz), ia_o, take(ptrs[2], ctypes.c_int32, nnz), perm

@@ -170,4 +170,32 @@ void matrixMarketToCSR(const char *filename, double **a, MKL_INT **ia, MKL_INT *
     }
 }
 
+// The file's base name without its extension (src/misc.c:254-281: the text
+// between the last '/' and the last '.' after it).  Where the reference returns
+// NULL (no extension) this returns the whole base name.  malloc'd; free().
+char *pathToMatrixName(const char *filepath) {
+    if (!filepath) return nullptr;
+    const char *base = strrchr(filepath, '/');
+    base = base ? base + 1 : filepath;
+    const char *dot = strrchr(base, '.');
+    const size_t len = dot ? (size_t)(dot - base) : strlen(base);
+    char *out = (char *)malloc(len + 1);
+    if (!out) return nullptr;
+    memcpy(out, base, len);
+    out[len] = '\0';
+    return out;
+}
+
+// str1 followed by str2 in a new malloc'd string (src/misc.c:283-297); a NULL
+// argument reads as the empty string.
+char *strconcat(const char *str1, const char *str2) {
+    const size_t l1 = str1 ? strlen(str1) : 0, l2 = str2 ? strlen(str2) : 0;
+    char *out = (char *)malloc(l1 + l2 + 1);
+    if (!out) return nullptr;
+    if (l1) memcpy(out, str1, l1);
+    if (l2) memcpy(out + l1, str2, l2);
+    out[l1 + l2] = '\0';
+    return out;
+}
+
 }  // extern "C"

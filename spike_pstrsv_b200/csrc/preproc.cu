@@ -618,9 +618,13 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     std::vector<Part> &parts = s->parts;
     parts.assign(P, Part{});
     if (starts && ends) {
+        // caller bounds are in the caller's row order: 'L' partition t, rows
+        // [starts[t], ends[t]) of L, is partition P-1-t of the mirror J L J
+        const bool lower = uplo == 'L' || uplo == 'l';
         for (int t = 0; t < P; t++) {
-            parts[t].ps = starts[t];
-            parts[t].pe = ends[t];
+            const int c = lower ? P - 1 - t : t;
+            parts[t].ps = lower ? n - ends[c] : starts[c];
+            parts[t].pe = lower ? n - starts[c] : ends[c];
         }
         for (int t = 0; t < P; t++) {
             bool ok = parts[t].pe > parts[t].ps && (t == 0 ? parts[t].ps == 0 : parts[t].ps == parts[t - 1].pe);
