@@ -1,8 +1,10 @@
 """Batched solves (many right-hand sides per launch) in FP64 and in FP32 with FP64
-iterative refinement, against single solves and the known solutions."""
+iterative refinement, against single solves, the sequential FP64 oracle and the
+known solutions."""
 import numpy as np
 import pytest
 
+import oracle
 import spike_pstrsv_b200 as spk
 from cases import rel_err
 from spike_pstrsv_b200 import synth
@@ -30,6 +32,7 @@ def test_batch_fp64_matches_single_solves(uplo, nrhs):
     assert r <= 1e-12
     for k in range(nrhs):
         assert rel_err(X[k], S.solve(B[k])) <= 1e-13
+        assert rel_err(X[k], oracle.sequential_solve(A, B[k], uplo)) <= 1e-12
         assert rel_err(X[k], Xt[k]) <= 1e-12
 
 
@@ -47,6 +50,7 @@ def test_batch_fp32_refinement_reaches_fp64_accuracy(uplo, nrhs):
     assert r <= 1e-12
     assert 1 <= it <= 4
     for k in range(nrhs):
+        assert rel_err(X[k], oracle.sequential_solve(A, B[k], uplo)) <= 1e-12
         assert rel_err(X[k], Xt[k]) <= 1e-12
 
 

@@ -1,9 +1,10 @@
 """Many systems in one captured launch sequence: every system's columns against
-x_true and against its own batched solve, FP64 and FP32 + refinement, graph
-replays, the autotuner, error paths."""
+x_true, the sequential FP64 oracle and its own batched solve, FP64 and FP32 +
+refinement, graph replays, the autotuner, error paths."""
 import numpy as np
 import pytest
 
+import oracle
 import spike_pstrsv_b200 as spk
 from spike_pstrsv_b200 import group, synth
 from spike_pstrsv_b200.capi import SpkError
@@ -44,6 +45,9 @@ def test_group_matches_each_system(mode, iters):
             ref = torch.zeros_like(B[i])
             systems[i].solve_batch(B[i], ref, mode=0, want_resid=False)
             assert _rel(xx, ref.cpu().numpy()) <= 1e-12
+            if rep == 0:
+                xo = np.stack([oracle.sequential_solve(mats[i], Bh[k], "L") for k in range(Bh.shape[0])])
+                assert _rel(xx, xo) <= 1e-12
     g.close()
 
 

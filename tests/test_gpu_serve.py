@@ -1,11 +1,13 @@
 """Serving loop: every result is the same alone and in a concurrent mix (scaled
-residual <= 1e-12, alone vs mix within 1e-12 relative), LRU eviction under a
+residual <= 1e-12, alone vs mix and against the sequential FP64 oracle within
+1e-12 relative), LRU eviction under a
 small HBM budget, continuous batching of queued requests, error paths."""
 import threading
 
 import numpy as np
 import pytest
 
+import oracle
 from spike_pstrsv_b200 import serve, synth
 from spike_pstrsv_b200.capi import SpkError
 
@@ -72,6 +74,8 @@ def test_results_are_the_same_alone_and_in_the_mix(mode):
             assert 0 <= r.scaled_residual <= TOL
         assert _rel(r.x, a) <= TOL
         assert _rel(r.x, Xt) <= 1e-11
+        xo = np.stack([oracle.sequential_solve(mats[mid], B[k], "L") for k in range(B.shape[0])])
+        assert _rel(r.x.reshape(xo.shape), xo) <= TOL
         assert r.latency_s > 0
     assert st["completed"] == 2 * len(reqs)
     assert st["preprocessings"] == len(mats)
