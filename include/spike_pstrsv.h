@@ -194,9 +194,10 @@ char *strconcat(const char *str1, const char *str2);
  * partition_starts/ends/numRows set and IS_MATRIX_PARTITIONED = 1 for the next
  * spike_pstrsv_preproc.  The partitioner replaces the reference's METIS k-way
  * call: a reverse Cuthill-McKee order of the pattern of A + A^T cut into
- * nthreads contiguous ranges of nearly equal nonzero count; rows are then
- * grouped by partition in their original order, as in the reference.  The
- * renumbering and triangle run on the GPU.
+ * nthreads contiguous ranges of nearly equal nonzero count; the rows are
+ * renumbered in that order (so each partition keeps the narrow band; the
+ * reference keeps a METIS part's rows in their original order).  The graph,
+ * the renumbering and the triangle are built on the GPU.
  * matrixAnalysis: 1 (and the matrix replaced by its triangle, re-read from
  * matrixFileName, or taken in memory when it is NULL) when no entry of the
  * triangle couples two equal partitions, else 0.
@@ -211,7 +212,7 @@ void matrixDuplication(int numRows, double *a, MKL_INT *ia, MKL_INT *ja, double 
                        MKL_INT **ja_dup);
 /* Status-returning reordering (no reference counterpart): matrixReordering's
  * renumbering and triangle without the matrixAnalysis shortcut; perm (optional,
- * n ints) receives the original row of every new row. */
+ * n ints) receives the original row of every new row (the RCM order). */
 int spk_reorder(double **a, int **ia, int **ja, int n, int nparts, char uplo, int *perm);
 /* The reordering's partitioner alone, host code (no GPU): order[q] = the row at
  * position q of the reverse Cuthill-McKee order, part[r] = the partition of row
@@ -303,6 +304,20 @@ int spk_chain_phase(spk_system *s, int phase, int row_lo, int row_hi, const doub
  * NULL) receives the bytes released.  SPK_ERR_STATE unless
  * spk_debug_scalar(s, "chain") == 1. */
 int spk_compact(spk_system *s, long long *freed);
+
+/* Tuning knobs of a system solved by chains (no reference counterpart; the
+ * reference's only knob is nthreads).  spk_debug_scalar(s, name) reads them back.
+ *   "rows":       rows per chain task of the one-right-hand-side solve (rounded
+ *                 up to whole 32-row tiles, doubled at most three times until
+ *                 every chain keeps its first rows final; SPK_ERR_ARG if none)
+ *   "batch_rows": the same for the batched solve's own chains
+ *   "stages":     2 or 3 tiles staged ahead by the one-right-hand-side kernel
+ *   "batch_path": 1 batched solves on the chain kernels, 0 on the partition
+ *                 kernels (not after spk_compact), -1 automatic (default)
+ * Preprocessing sets the defaults again.  Not concurrent with the system's
+ * solves: the device is synchronized before task lists are replaced.
+ * SPK_ERR_STATE unless spk_debug_scalar(s, "chain") == 1. */
+int spk_tune(spk_system *s, const char *name, long long value);
 
 /* Test hook (no reference counterpart): spk_debug_set(s, "fail_waits", 1) makes
  * every solve kernel of s report a failed bounded wait at entry, before it

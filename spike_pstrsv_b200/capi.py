@@ -317,6 +317,15 @@ class System:
         _check(lib().spk_compact(self.h, ctypes.byref(freed)))
         return int(freed.value)
 
+    def tune(self, name: str, value: int) -> "System":
+        """Chain-solver knobs (spk_tune): "rows" and "batch_rows" (rows per chain
+        task of the one-right-hand-side and batched solves), "stages" (2 or 3 tiles
+        staged ahead), "batch_path" (1 chain, 0 partition kernels, -1 automatic)."""
+        L = lib()
+        L.spk_tune.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_longlong]
+        _check(L.spk_tune(self.h, name.encode(), int(value)))
+        return self
+
     def debug_set(self, name: str, value: int) -> "System":
         """Test hooks (spk_debug_set): "fail_waits" makes the solve kernels report a
         failed bounded wait until the failure has been reported once."""

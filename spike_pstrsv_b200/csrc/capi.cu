@@ -525,6 +525,18 @@ int spk_set_truncation(spk_system *s, double tau) {
     return SPK_OK;
 }
 
+int spk_tune(spk_system *s, const char *name, long long value) {
+    if (!s || !name) {
+        set_error(SPK_ERR_ARG, "null argument");
+        return SPK_ERR_ARG;
+    }
+    if (!s->built) {
+        set_error(SPK_ERR_STATE, "spk_tune needs a preprocessed system");
+        return SPK_ERR_STATE;
+    }
+    return spk::chain_tune(s, name, value);
+}
+
 int spk_compact(spk_system *s, long long *freed) {
     if (!s) {
         set_error(SPK_ERR_ARG, "null argument");
@@ -601,6 +613,11 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "chain_rows_phase4")) return s->ch_rows4;
     if (!strcmp(name, "chain_tasks_phase4")) return s->nctasks4;
     if (!strcmp(name, "chain_batch_rows")) return s->cp_batch.len ? s->cp_batch.len : s->ch_len;
+    // spk_tune's knobs under their own names
+    if (!strcmp(name, "rows")) return s->ch_len;
+    if (!strcmp(name, "batch_rows")) return s->cp_batch.len ? s->cp_batch.len : s->ch_len;
+    if (!strcmp(name, "stages")) return s->ch_stages;
+    if (!strcmp(name, "batch_path")) return s->batch_path;
     if (!strcmp(name, "chain_host_rows")) return s->cp_host.len ? s->cp_host.len : s->ch_len;
     if (!strcmp(name, "chain_bytes")) return (long long)(s->ch_val.bytes() + s->ch_off.bytes() + s->ch_ptr.bytes());
     if (!strcmp(name, "rows_phase4")) return s->rows_phase4;

@@ -998,6 +998,7 @@ int chain_batch_values(spk_system *s, int fp32) {
 
 void chain_release(spk_system *s) {
     s->chain_ok = 0;
+    s->batch_path = -1;
     s->ch_val.release();
     s->ch_valb.release();
     s->ch_valbf.release();
@@ -1406,6 +1407,106 @@ int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool
         cudaEventRecord(s->ev[ring][2], st);
     }
     SPK_TRY(launch_chain<true>(s, s->d_ctasks4.p, s->nctasks4, b, x, st));
+    return SPK_OK;
+}
+
+// Tuning knobs of a system solved by chains (spk_tune).  A changed plan or stage
+// count drops the captured host-array pipeline (it holds the old launches); the
+// caller keeps the system's solves off the GPU meanwhile (the device is
+// synchronized before task lists are replaced).
+int chain_tune(spk_system *s, const char *name, long long v) {
+    if (!s->chain_ok) {
+        set_error(SPK_ERR_STATE, "spk_tune needs a system solved by chains");
+        return SPK_ERR_STATE;
+    }
+    auto drop_pipeline = [&]() {
+        if (s->pipe_exec) cudaGraphExecDestroy(s->pipe_exec);
+        s->pipe_exec = nullptr;
+        s->pipe_b = s->pipe_db = nullptr;
+        s->pipe_x = s->pipe_dx = nullptr;
+        s->pipe_K = 0;
+    };
+    if (!strcmp(name, "stages")) {  // tiles staged by the one-right-hand-side kernel
+        if (v != 2 && v != 3) {
+            set_error(SPK_ERR_ARG, "stages must be 2 or 3 (got %lld)", v);
+            return SPK_ERR_ARG;
+        }
+        SPK_CUDA(cudaDeviceSynchronize());
+        s->ch_stages = (int)v;
+        drop_pipeline();
+        return SPK_OK;
+    }
+    if (!strcmp(name, "batch_path")) {  // 1 chain kernels, 0 partition kernels, -1 automatic
+        if (v < -1 || v > 1 || (v == 0 && s->lean)) {
+            set_error(SPK_ERR_ARG, "batch_path must be -1, 0 or 1 (0 needs the partition pools: not compacted)");
+            return SPK_ERR_ARG;
+        }
+        s->batch_path = (int)v;
+        return SPK_OK;
+    }
+    const bool plain = !strcmp(name, "rows");
+    if (!plain && strcmp(name, "batch_rows")) {
+        set_error(SPK_ERR_ARG, "unknown tuning knob '%s' (rows, batch_rows, stages, batch_path)", name);
+        return SPK_ERR_ARG;
+    }
+    // rows per chain task, whole tiles; build_plan doubles the length (at most
+    // three times) until every chain keeps its first rows final
+    if (v < 32 || v > s->n) {
+        set_error(SPK_ERR_ARG, "%s must be in [32, n] (got %lld)", name, v);
+        return SPK_ERR_ARG;
+    }
+    const long long len = 32ll * ((v + 31) / 32);
+    ChainPlan fresh;
+    const int keep_len = s->ch_len;
+    s->ch_len = 0;  // so that build_plan builds the extra plan even at the plain length
+    const int rc = build_plan(s, len, s->ch_reach, &fresh);
+    s->ch_len = keep_len;
+    SPK_TRY(rc);
+    if (!fresh.len) {
+        set_error(SPK_ERR_ARG, "no chain length from %lld rows keeps every chain's first rows final", len);
+        return SPK_ERR_ARG;
+    }
+    SPK_CUDA(cudaDeviceSynchronize());
+    if (!plain) {
+        s->cp_batch.release();
+        s->cp_batch.d1.p = fresh.d1.p, s->cp_batch.d1.n = fresh.d1.n, fresh.d1.p = nullptr;
+        s->cp_batch.d4.p = fresh.d4.p, s->cp_batch.d4.n = fresh.d4.n, fresh.d4.p = nullptr;
+        s->cp_batch.h1.swap(fresh.h1);
+        s->cp_batch.h4.swap(fresh.h4);
+        s->cp_batch.len = fresh.len;
+        return SPK_OK;
+    }
+    // the plain plan: keep the batched solve on its own chains (it used the plain
+    // ones when it had no plan of its own)
+    if (!s->cp_batch.len) {
+        ChainPlan old;
+        old.h1 = s->h_ctasks1;
+        old.h4 = s->h_ctasks4;
+        SPK_TRY(upload_vec(old.d1, old.h1));
+        SPK_TRY(upload_vec(old.d4, old.h4));
+        old.len = s->ch_len;
+        s->cp_batch.d1.p = old.d1.p, s->cp_batch.d1.n = old.d1.n, old.d1.p = nullptr;
+        s->cp_batch.d4.p = old.d4.p, s->cp_batch.d4.n = old.d4.n, old.d4.p = nullptr;
+        s->cp_batch.h1.swap(old.h1);
+        s->cp_batch.h4.swap(old.h4);
+        s->cp_batch.len = old.len;
+    }
+    s->d_ctasks1.release();
+    s->d_ctasks4.release();
+    s->d_ctasks1.p = fresh.d1.p, s->d_ctasks1.n = fresh.d1.n, fresh.d1.p = nullptr;
+    s->d_ctasks4.p = fresh.d4.p, s->d_ctasks4.n = fresh.d4.n, fresh.d4.p = nullptr;
+    long long rows1 = 0, rows4 = 0;
+    for (const ChainTask &t : fresh.h1) rows1 += t.hi - t.lo;
+    for (const ChainTask &t : fresh.h4) rows4 += t.hi - t.lo;
+    s->h_ctasks1.swap(fresh.h1);
+    s->h_ctasks4.swap(fresh.h4);
+    s->nctasks1 = (int)s->h_ctasks1.size();
+    s->nctasks4 = (int)s->h_ctasks4.size();
+    s->ch_rows1 = rows1;
+    s->ch_rows4 = rows4;
+    s->ch_count = s->nctasks1;
+    s->ch_len = fresh.len;
+    drop_pipeline();
     return SPK_OK;
 }
 

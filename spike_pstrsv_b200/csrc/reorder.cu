@@ -11,21 +11,28 @@
 // the next preprocessing as caller-set partitions (IS_MATRIX_PARTITIONED).
 // METIS is not part of this library, so the partitioner is a bandwidth-driven
 // one: a reverse Cuthill-McKee ordering of the same graph (per connected
-// component from a pseudo-peripheral node found by the George-Liu iteration,
+// component from a pseudo-peripheral node found by the George-Liu iteration
+// started at the component's lightest node,
 // neighbours taken in increasing degree, ties by index), cut into nthreads
 // contiguous ranges of nearly equal nonzero count; part k is range k.  Rows
 // that are close in an RCM order are close in the matrix, so a part touches only
 // the parts beside it: for the triangle that the Spike solve runs on, a block
-// couples to the next block alone, through the rows at the boundary.
-// Every step after the partition vector is the reference's: rows grouped by
-// part in original order, the permuted matrix as CSR with sorted columns
-// (:174-190, mkl_dcsrcoo job 2), the upper or lower triangle (:192-264), the
-// partition bounds from the part sizes (:266-276).
+// couples to the next block alone, through the rows at the boundary.  The rows
+// are renumbered in the RCM order (grouped by part, the band kept inside each
+// part; the reference keeps a METIS part's rows in their original order).
+// The steps after that are the reference's: the permuted matrix as CSR with
+// sorted columns (:174-190, mkl_dcsrcoo job 2), the upper or lower triangle
+// (:192-264), the partition bounds from the part sizes (:266-276).  The
+// reference's matrixReordering given the RCM-ordered matrix and these
+// contiguous parts produces the same arrays.
 //
-// The graph and the ordering are built on the host (breadth-first search is
-// sequential); the O(nnz) part - permuting every entry, sorting by (row,
-// column), dropping the other triangle, row pointers - runs on the GPU: one
-// 64-bit key per entry, a CUB radix sort over the bits the keys use.
+// The O(nnz) steps run on the GPU with one 64-bit key per entry and a CUB radix
+// sort over the bits the keys use: the graph (both orientations of every
+// off-diagonal entry, sorted, repeats removed), and after the ordering the
+// permuted triangle (every entry renumbered, sorted by (row, column), the other
+// triangle dropped, row pointers by binary search).  The ordering itself runs
+// on the host: breadth-first search is sequential.  spk_reorder_plan builds the
+// same graph on the host, for planning without a GPU.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -157,6 +164,8 @@ inline bool lighter(const Graph &g, int x, int y) {  // degree, then index
 
 // George-Liu: from the lightest node of the component, move to the lightest
 // node of the last breadth-first level while that lengthens the level structure.
+// (Starting at the component's first node instead saves one search but left
+// wider bands, e.g. 149 against 103 rows on a scrambled banded matrix.)
 int pseudo_peripheral(const Graph &g, int s0, Stamps &st) {
     Levels lv, lx;
     bfs(g, s0, st, lv);
@@ -226,18 +235,21 @@ void cut(int n, const int *ia, const std::vector<int> &order, int nparts, std::v
         for (int p = bound[k]; p < bound[k + 1]; ++p) part[order[p]] = k;
 }
 
-int plan(int n, const int *ia, const int *ja, int nparts, std::vector<int> &order, std::vector<int> &part) {
+int check_plan_args(int n, const int *ia, const int *ja, int nparts) {
     SPK_TRY(check_csr(n, ia, ja));
     if (nparts <= 0 || nparts > n || nparts > SPK_MAX_EXPORTED_PARTS) {
         set_error(SPK_ERR_ARG, "reordering: %d parts for %d rows (1..min(n, %d))", nparts, n,
                   SPK_MAX_EXPORTED_PARTS);
         return SPK_ERR_ARG;
     }
-    Graph g;
-    symmetric_pattern(n, ia, ja, g);
+    return SPK_OK;
+}
+
+// The partitioner on a graph built by the caller (host or GPU pattern: the same
+// sorted, repeat-free rows).
+void plan_on(const Graph &g, int n, const int *ia, int nparts, std::vector<int> &order, std::vector<int> &part) {
     rcm(g, n, order);
     cut(n, ia, order, nparts, part);
-    return SPK_OK;
 }
 
 // --------------------------------------------------------------------------
@@ -291,6 +303,45 @@ __global__ void k_gather_entries(I64 kept, const unsigned long long *__restrict_
     }
 }
 
+// Pattern of A + A^T on the GPU: both orientations of every off-diagonal entry
+// as keys row << 32 | column (diagonal entries: n << 32, sorted last), radix
+// sort, unique.  One warp per row.
+__global__ void k_sym_keys(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                           unsigned long long *__restrict__ keys) {
+    const int lane = threadIdx.x & 31;
+    const I64 w0 = ((I64)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const I64 nw = ((I64)gridDim.x * blockDim.x) >> 5;
+    const unsigned long long drop = (unsigned long long)(unsigned)n << 32;
+    for (I64 r = w0; r < n; r += nw) {
+        const int e = ia[r + 1];
+        for (int k = ia[r] + lane; k < e; k += 32) {
+            const unsigned c = (unsigned)ja[k];
+            const bool off = c != (unsigned)r;
+            keys[2 * (I64)k] = off ? (((unsigned long long)r << 32) | c) : drop;
+            keys[2 * (I64)k + 1] = off ? (((unsigned long long)c << 32) | (unsigned)r) : drop;
+        }
+    }
+}
+
+// p[r] = first key of row r (binary search), r = 0..n; p[n] = count.
+__global__ void k_row_ptr64(int n, const unsigned long long *__restrict__ keys, I64 count, I64 *__restrict__ p) {
+    for (I64 r = (I64)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += (I64)gridDim.x * blockDim.x) {
+        const unsigned long long t = (unsigned long long)r << 32;
+        I64 lo = 0, hi = count;
+        while (lo < hi) {
+            const I64 mid = (lo + hi) >> 1;
+            if (keys[mid] < t) lo = mid + 1;
+            else hi = mid;
+        }
+        p[r] = lo;
+    }
+}
+
+__global__ void k_key_cols(I64 count, const unsigned long long *__restrict__ keys, int *__restrict__ j) {
+    for (I64 k = (I64)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (I64)gridDim.x * blockDim.x)
+        j[k] = (int)(unsigned)(keys[k] & 0xffffffffull);
+}
+
 template <typename T>
 T *host_alloc(size_t count) {
     void *p = nullptr;
@@ -303,6 +354,72 @@ int grid_for(I64 work, int threads) {
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const I64 want = (work + threads - 1) / threads;
     return (int)std::max<I64>(1, std::min<I64>(want, (I64)sms * 16));
+}
+
+int row_bits_for(int n) {
+    int b = 1;
+    while (b < 31 && (1u << b) <= (unsigned)n) ++b;
+    return b;
+}
+
+// The graph of the partitioner (pattern of A + A^T without the diagonal) built
+// on the GPU from the host CSR; the same rows as symmetric_pattern.
+int symmetric_pattern_gpu(int n, const int *ia, const int *ja, Graph &g) {
+    const I64 nnz = ia[n];
+    cudaStream_t st = nullptr;
+    SPK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int rc = SPK_OK;
+    {
+        DBuf<int> d_ia(st), d_ja(st), d_j(st);
+        DBuf<unsigned long long> d_keys(st), d_sorted(st), d_uniq(st);
+        DBuf<I64> d_p(st), d_count(st);
+        DBuf<unsigned char> d_tmp(st);
+        auto run = [&]() -> int {
+            SPK_TRY(d_ia.alloc(n + 1));
+            SPK_TRY(d_ja.alloc(nnz));
+            SPK_TRY(d_keys.alloc(2 * nnz));
+            SPK_CUDA(cudaMemcpyAsync(d_ia.p, ia, sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st));
+            SPK_CUDA(cudaMemcpyAsync(d_ja.p, ja, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
+            k_sym_keys<<<grid_for((I64)n * 32, 256), 256, 0, st>>>(n, d_ia.p, d_ja.p, d_keys.p);
+            SPK_CUDA(cudaGetLastError());
+            d_ja.release();
+            SPK_TRY(d_sorted.alloc(2 * nnz));
+            const int end_bit = 32 + row_bits_for(n);
+            size_t t1 = 0, t2 = 0;
+            SPK_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, t1, d_keys.p, d_sorted.p, 2 * nnz, 0, end_bit, st));
+            SPK_CUDA(cub::DeviceSelect::Unique(nullptr, t2, d_sorted.p, d_keys.p, d_count.p, 2 * nnz, st));
+            SPK_TRY(d_tmp.alloc(std::max(t1, t2)));
+            SPK_TRY(d_count.alloc(1));
+            SPK_CUDA(cub::DeviceRadixSort::SortKeys(d_tmp.p, t1, d_keys.p, d_sorted.p, 2 * nnz, 0, end_bit, st));
+            SPK_CUDA(cub::DeviceSelect::Unique(d_tmp.p, t2, d_sorted.p, d_keys.p, d_count.p, 2 * nnz, st));
+            I64 count = 0;
+            SPK_CUDA(cudaMemcpyAsync(&count, d_count.p, sizeof(I64), cudaMemcpyDeviceToHost, st));
+            SPK_CUDA(cudaStreamSynchronize(st));
+            // unique keys in d_keys; the diagonal's key (row n), if any, is last
+            d_sorted.release();
+            d_tmp.release();
+            SPK_TRY(d_p.alloc(n + 1));
+            k_row_ptr64<<<grid_for((I64)n + 1, 256), 256, 0, st>>>(n, d_keys.p, count, d_p.p);
+            SPK_CUDA(cudaGetLastError());
+            g.p.assign(n + 1, 0);
+            SPK_CUDA(cudaMemcpyAsync(g.p.data(), d_p.p, sizeof(I64) * (n + 1), cudaMemcpyDeviceToHost, st));
+            SPK_CUDA(cudaStreamSynchronize(st));
+            const I64 edges = g.p[n];  // entries of rows < n: the diagonal's key excluded
+            SPK_TRY(d_j.alloc(edges));
+            if (edges) {
+                k_key_cols<<<grid_for(edges, 256), 256, 0, st>>>(edges, d_keys.p, d_j.p);
+                SPK_CUDA(cudaGetLastError());
+            }
+            g.j.resize(edges);
+            if (edges) SPK_CUDA(cudaMemcpyAsync(g.j.data(), d_j.p, sizeof(int) * edges, cudaMemcpyDeviceToHost, st));
+            SPK_CUDA(cudaStreamSynchronize(st));
+            return SPK_OK;
+        };
+        rc = run();
+    }
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
 }
 
 // The triangle of P A P^T (P: row i of the result is row perm[i] of A) as a new
@@ -339,9 +456,7 @@ int permute_triangle(int n, const double *a, const int *ia, const int *ja, const
                                                                       d_keys.p, d_idx.p, d_kept.p);
             SPK_CUDA(cudaGetLastError());
             // rows need the bits of n (the dropped entries' row), columns 32 bits
-            int row_bits = 1;
-            while (row_bits < 31 && (1u << row_bits) <= (unsigned)n) ++row_bits;
-            const int end_bit = 32 + row_bits;
+            const int end_bit = 32 + row_bits_for(n);
             size_t tmp = 0;
             SPK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d_keys.p, d_keys2.p, d_idx.p, d_idx2.p, nnz, 0,
                                                      end_bit, st));
@@ -446,13 +561,22 @@ int reorder(double **a, int **ia, int **ja, int n, int nparts, char uplo, std::v
         set_error(SPK_ERR_ARG, "reordering: null matrix");
         return SPK_ERR_ARG;
     }
+    SPK_TRY(check_plan_args(n, *ia, *ja, nparts));
     std::vector<int> order, part;
-    SPK_TRY(plan(n, *ia, *ja, nparts, order, part));
-    // rows grouped by part, original order inside a part (src/matrix_reordering.c:152-172)
-    std::vector<int> sizes(nparts, 0), first(nparts + 1, 0), perm(n), iperm(n);
+    {
+        Graph g;
+        SPK_TRY(symmetric_pattern_gpu(n, *ia, *ja, g));
+        plan_on(g, n, *ia, nparts, order, part);
+    }
+    // Rows in RCM order: the partitions are ranges of it, so the rows are grouped
+    // by partition (src/matrix_reordering.c:152-172) and keep the narrow band
+    // inside each one.  (The reference keeps the original order inside a METIS
+    // part; inside an RCM range that order can be arbitrary - a scrambled input
+    // stays scrambled - and the dense spikes of the next preprocessing grow with
+    // the partition's width.)
+    std::vector<int> sizes(nparts, 0), iperm(n);
     for (int v = 0; v < n; ++v) sizes[part[v]]++;
-    for (int t = 0; t < nparts; ++t) first[t + 1] = first[t] + sizes[t];
-    for (int v = 0; v < n; ++v) perm[first[part[v]]++] = v;
+    const std::vector<int> &perm = order;
     for (int i = 0; i < n; ++i) iperm[perm[i]] = i;
     const char u = (char)toupper((unsigned char)uplo);
     double *ao = nullptr;
@@ -466,7 +590,7 @@ int reorder(double **a, int **ia, int **ja, int n, int nparts, char uplo, std::v
     *ja = jo;
     set_bounds(sizes);
     IS_MATRIX_PARTITIONED = 1;
-    if (perm_out) perm_out->swap(perm);
+    if (perm_out) *perm_out = perm;
     return SPK_OK;
 }
 
@@ -474,10 +598,17 @@ int reorder(double **a, int **ia, int **ja, int n, int nparts, char uplo, std::v
 
 extern "C" {
 
-// Host-only plan (no GPU): the RCM order and the part of every row.
+// The partitioner alone, host code (no GPU; the graph is built on the host,
+// where matrixReordering builds the same graph on the GPU): the RCM order and
+// the part of every row.
 int spk_reorder_plan(int n, const int *ia, const int *ja, int nparts, int *order, int *part) {
+    SPK_TRY(spk::check_plan_args(n, ia, ja, nparts));
     std::vector<int> o, p;
-    SPK_TRY(spk::plan(n, ia, ja, nparts, o, p));
+    {
+        spk::Graph g;
+        spk::symmetric_pattern(n, ia, ja, g);
+        spk::plan_on(g, n, ia, nparts, o, p);
+    }
     if (order) std::copy(o.begin(), o.end(), order);
     if (part) std::copy(p.begin(), p.end(), part);
     return SPK_OK;

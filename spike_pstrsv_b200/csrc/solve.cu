@@ -2336,7 +2336,9 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     // count measured); FP32 + refinement: the chain kernel when the partitions give
     // too few tasks to fill the GPU
     const char *cb = getenv("SPK_CHAIN_BATCH");  // 1: always the chain kernels, 0: never
-    const bool use_chain = s->chain_ok && (s->lean || (cb ? cb[0] == '1' : (mode == 0 || !part_wide)));
+    const bool use_chain =
+        s->chain_ok && (s->lean || (s->batch_path >= 0 ? s->batch_path == 1
+                                                       : (cb ? cb[0] == '1' : (mode == 0 || !part_wide))));
     if (use_chain) {
         // the chain tasks fill the GPU whatever the partition count: every group
         // of up to 32 columns is one right-hand-side-parallel chain solve (used

@@ -191,6 +191,7 @@ struct spk_system {
     spk::DBuf<spk::ChainTask> d_ctasks1, d_ctasks4;
     spk::ChainPlan cp_batch;  // the batched kernel's own chains (longer; built at preprocessing)
     spk::ChainPlan cp_host;   // the host-array pipeline's chains (shorter; built on first use)
+    int batch_path = -1;      // spk_tune "batch_path": 1 chain kernels, 0 partition kernels, -1 automatic
     int host_plan_tried = 0;
     int nctasks1 = 0, nctasks4 = 0;
     long long ch_rows1 = 0, ch_rows4 = 0;
@@ -234,6 +235,7 @@ int solve_batch_static(spk_system *s, int nrhs, const double *B, long long ldb, 
 int solve_prepare(spk_system *s);
 int residual_prepare(spk_system *s);
 int chain_prepare(spk_system *s);
+int chain_tune(spk_system *s, const char *name, long long v);
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);
 long long chain_device_check();

@@ -1,5 +1,6 @@
 """Test checker: a plain-Python restatement of the reordering's partitioner
 (reverse Cuthill-McKee from a George-Liu pseudo-peripheral node per component,
+searched from the component's lightest node,
 neighbours by increasing degree then index, cut into ranges of nearly equal row
 nonzeros) and of the reference's later steps (src/matrix_reordering.c:152-264:
 rows grouped by partition in original order, the permuted matrix's triangle as

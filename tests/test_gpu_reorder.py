@@ -1,9 +1,10 @@
 """Partition-aware reordering on the GPU (matrixReordering / spk_reorder, the
 role of src/matrix_reordering.c:83-305) against the reference's own reordering
-steps (oracle/_ref, its METIS call answered with the same partition) and the
-checker restatement; then the Spike preprocessing and solve of the reordered
-triangle with the reordering's partitions (IS_MATRIX_PARTITIONED) against the
-reference's.  Structure bit-identical, x to relative error <= 1e-12."""
+steps (oracle/_ref: its matrixReordering given the RCM-ordered matrix, its METIS
+call answered with the same contiguous partitions) and the checker restatement;
+then the Spike preprocessing and solve of the reordered triangle with the
+reordering's partitions (IS_MATRIX_PARTITIONED) against the reference's.
+Structure bit-identical, x to relative error <= 1e-12."""
 import numpy as np
 import pytest
 
@@ -26,10 +27,12 @@ def test_reorder_matches_restatement(name, uplo):
     F = Csr(A)
     P = 6
     a, ia, ja, perm = spk.reorder(F.a, F.ia, F.ja, F.m, P, uplo)
-    _, part = spk.reorder_plan(F.ia, F.ja, F.m, P)
-    perm_ref, _ = grouped_perm(part, P)
-    assert np.array_equal(perm, perm_ref)
-    ra, ria, rja = permuted_triangle(A, perm_ref, uplo)
+    order, part = spk.reorder_plan(F.ia, F.ja, F.m, P)  # the host-built graph gives the same plan
+    assert np.array_equal(perm, order)
+    perm_ref, sizes = grouped_perm(part[order], P)  # parts are ranges of the order: grouping keeps it
+    assert np.array_equal(perm_ref, np.arange(F.m))
+    assert [spk.get_global("partition_numRows", t) for t in range(P)] == list(sizes)
+    ra, ria, rja = permuted_triangle(A, order, uplo)
     assert np.array_equal(ia, ria) and np.array_equal(ja, rja)
     assert np.array_equal(a.view(np.uint64), ra.view(np.uint64))
     assert spk.get_flag("IS_MATRIX_PARTITIONED") == 1
@@ -42,9 +45,10 @@ def test_reorder_matches_restatement(name, uplo):
 def test_matrix_reordering_matches_reference(uplo, P):
     A = scrambled(grid(40), 11)
     F = Csr(A)
-    _, part = spk.reorder_plan(F.ia, F.ja, F.m, P)
+    order, part = spk.reorder_plan(F.ia, F.ja, F.m, P)
     R = oracle.Reference()
-    ra, ria, rja, rs, re, rn = R.reorder(F, P, uplo, part)
+    # the reference's steps on the RCM-ordered matrix with the same (contiguous) parts
+    ra, ria, rja, rs, re, rn = R.reorder(Csr(A[order][:, order]), P, uplo, part[order])
     R.set_flag("IS_MATRIX_PARTITIONED", 0)
     a, ia, ja, _ = spk.reorder(F.a, F.ia, F.ja, F.m, P, uplo, legacy=True)
     assert spk.get_flag("IS_MATRIX_PARTITIONED") == 1
@@ -62,9 +66,9 @@ def test_reordered_system_solves_as_reference(P):
     reference's profiler drives it with METIS (test/runtime_analysis.c:297-310, 413-427)."""
     A = scrambled(grid(48), 12)
     F = Csr(A)
-    _, part = spk.reorder_plan(F.ia, F.ja, F.m, P)
+    order, part = spk.reorder_plan(F.ia, F.ja, F.m, P)
     R = oracle.Reference()
-    ra, ria, rja, *_ = R.reorder(F, P, "U", part)
+    ra, ria, rja, *_ = R.reorder(Csr(A[order][:, order]), P, "U", part[order])
 
     class U:
         a, ia, ja, m = ra, ria, rja, F.m
