@@ -613,6 +613,12 @@ long long spk_debug_scalar(const spk_system *s, const char *name) {
     if (!strcmp(name, "chain_rows_phase4")) return s->ch_rows4;
     if (!strcmp(name, "chain_tasks_phase4")) return s->nctasks4;
     if (!strcmp(name, "chain_batch_rows")) return s->cp_batch.len ? s->cp_batch.len : s->ch_len;
+    // wall microseconds of the last preprocessing, by part
+    if (!strncmp(name, "prep_us_", 8)) {
+        static const char *parts[5] = {"reference", "spikes", "tasks", "ell", "chains"};
+        for (int i = 0; i < 5; ++i)
+            if (!strcmp(name + 8, parts[i])) return (long long)(s->prep_ms[i] * 1e3);
+    }
     // spk_tune's knobs under their own names
     if (!strcmp(name, "rows")) return s->ch_len;
     if (!strcmp(name, "batch_rows")) return s->cp_batch.len ? s->cp_batch.len : s->ch_len;

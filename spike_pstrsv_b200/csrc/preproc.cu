@@ -544,6 +544,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     s->anorm = 0.0;
     s->ell_reach = -1;
     PhaseClock clk(ph, st);
+    const double prep_t0 = now_s();
 
     // ---- input: upload (host pointers) and mirror ('L')
     int nnz = 0;
@@ -1006,6 +1007,7 @@ int preprocess(spk_system *s, const double *a, const int *ia, const int *ja, int
     }
     SPK_CUDA(cudaStreamSynchronize(st));
     clk.lap(7);  // produceReducedSystem
+    s->prep_ms[0] = (now_s() - prep_t0) * 1e3;
 
     SPK_TRY(solve_prepare(s));
     s->built = 1;

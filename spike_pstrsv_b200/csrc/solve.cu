@@ -29,6 +29,7 @@
 // uplo='L' (x_L[i] = x_U[n-1-i]) is folded into the right-hand-side loads and
 // the solution stores.
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -1730,82 +1731,69 @@ int upload(DBuf<T> &d, const std::vector<T> &h) {
 
 }  // namespace
 
-int solve_prepare(spk_system *s) {
+// Internal spikes (no counterpart in the reference): coupled blocks the
+// reference gives no spike, whose phase-4 range would otherwise not be
+// truncated, get the spike of their coupling columns (a one-CTA sweep per
+// block); aux_first[t] >= 0: rows [ps, ps + aux_first[t]) keep y.
+int aux_spikes(spk_system *s, std::vector<int> &aux_first) {
     const int P = s->P;
     const double tau = s->trunc_tol;
-    // first significant spike row per split block (rows above it: x = y)
-    std::vector<int> first(P, 0);
-    {
-        std::vector<int> plist, nr(P), nc(P);
-        std::vector<long long> ss(P);
-        for (int t = 0; t < P; t++) {
-            const Part &p = s->parts[t];
-            nr[t] = p.nRowsS;
-            nc[t] = p.nColsS;
-            ss[t] = p.startsS;
-            first[t] = p.nRowsS;
-            if (p.hasS && p.nRowsS > 0) plist.push_back(t);
+    aux_first.assign(P, -1);
+    std::vector<int> hia(s->n + 1);
+    bool have_ia = false;
+    for (int t = 0; t < P; t++) {
+        const Part &p = s->parts[t];
+        const bool split = p.hasRefl || p.isOpt;
+        const bool banded_trunc = split && p.hasS && p.nRowsS > 0;
+        const int rl = p.maxIR;  // last row with a coupling column
+        if (banded_trunc || rl < p.ps || rl + 1 - p.ps < 256 || p.pe >= s->n) continue;
+        if (!have_ia) {
+            SPK_CUDA(cudaMemcpy(hia.data(), s->uia.p, sizeof(int) * (s->n + 1), cudaMemcpyDeviceToHost));
+            have_ia = true;
         }
-        if (tau >= 0 && !plist.empty()) {
-            DBuf<int> d_pl(s->stream), d_nr(s->stream), d_nc(s->stream), d_first(s->stream);
-            DBuf<long long> d_ss(s->stream);
-            SPK_TRY(upload(d_pl, plist));
-            SPK_TRY(upload(d_nr, nr));
-            SPK_TRY(upload(d_nc, nc));
-            SPK_TRY(upload(d_ss, ss));
-            SPK_TRY(upload(d_first, first));
-            dim3 grid(8, (unsigned)plist.size());
-            k_first_significant<<<grid, 256, 0, s->stream>>>((int)plist.size(), d_pl.p, d_ss.p, d_nr.p, d_nc.p,
-                                                              s->S.p, tau, d_first.p);
-            SPK_CUDA(cudaGetLastError());
-            SPK_CUDA(cudaStreamSynchronize(s->stream));
-            SPK_CUDA(cudaMemcpy(first.data(), d_first.p, sizeof(int) * P, cudaMemcpyDeviceToHost));
-        } else {
-            for (int t = 0; t < P; t++) first[t] = 0;
-        }
+        // distinct coupling columns of rows [ps, rl]
+        const int e0 = hia[p.ps], e1 = hia[rl + 1];
+        std::vector<int> hja(e1 - e0);
+        SPK_CUDA(cudaMemcpy(hja.data(), s->uja.p + e0, sizeof(int) * (e1 - e0), cudaMemcpyDeviceToHost));
+        std::vector<int> cols;
+        for (int c : hja)
+            if (c >= p.pe) cols.push_back(c);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        if (cols.empty() || cols.size() > 1024) continue;
+        const int rows = rl + 1 - p.ps, nc = (int)cols.size();
+        DBuf<int> d_cols(s->stream), d_first(s->stream);
+        DBuf<double> W(s->stream);
+        SPK_TRY(upload(d_cols, cols));
+        SPK_TRY(W.alloc((size_t)rows * nc));
+        SPK_TRY(d_first.alloc(1));
+        SPK_CUDA(cudaMemcpyAsync(d_first.p, &rows, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+        k_aux_sweep<<<1, ((nc + 31) / 32) * 32, 0, s->stream>>>(p.ps, rl, p.pe, s->uia.p, s->uja.p, s->ua.p,
+                                                                d_cols.p, nc, W.p);
+        k_aux_first<<<blocks_for(rows), 256, 0, s->stream>>>(rows, nc, W.p, tau, d_first.p);
+        SPK_CUDA(cudaGetLastError());
+        SPK_CUDA(cudaStreamSynchronize(s->stream));  // the stream does not sync with cudaMemcpy
+        int f = rows;
+        SPK_CUDA(cudaMemcpy(&f, d_first.p, sizeof(int), cudaMemcpyDeviceToHost));
+        aux_first[t] = f;
     }
-    // internal spikes: coupled blocks whose phase-4 range would not be truncated
-    std::vector<int> aux_first(P, -1);  // >= 0: rows [ps, ps+aux_first) keep y
-    if (tau >= 0 && s->redNec) {
-        std::vector<int> hia(s->n + 1);
-        bool have_ia = false;
-        for (int t = 0; t < P; t++) {
-            const Part &p = s->parts[t];
-            const bool split = p.hasRefl || p.isOpt;
-            const bool banded_trunc = split && p.hasS && p.nRowsS > 0;
-            const int rl = p.maxIR;  // last row with a coupling column
-            if (banded_trunc || rl < p.ps || rl + 1 - p.ps < 256 || p.pe >= s->n) continue;
-            if (!have_ia) {
-                SPK_CUDA(cudaMemcpy(hia.data(), s->uia.p, sizeof(int) * (s->n + 1), cudaMemcpyDeviceToHost));
-                have_ia = true;
-            }
-            // distinct coupling columns of rows [ps, rl]
-            const int e0 = hia[p.ps], e1 = hia[rl + 1];
-            std::vector<int> hja(e1 - e0);
-            SPK_CUDA(cudaMemcpy(hja.data(), s->uja.p + e0, sizeof(int) * (e1 - e0), cudaMemcpyDeviceToHost));
-            std::vector<int> cols;
-            for (int c : hja)
-                if (c >= p.pe) cols.push_back(c);
-            std::sort(cols.begin(), cols.end());
-            cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-            if (cols.empty() || cols.size() > 1024) continue;
-            const int rows = rl + 1 - p.ps, nc = (int)cols.size();
-            DBuf<int> d_cols(s->stream), d_first(s->stream);
-            DBuf<double> W(s->stream);
-            SPK_TRY(upload(d_cols, cols));
-            SPK_TRY(W.alloc((size_t)rows * nc));
-            SPK_TRY(d_first.alloc(1));
-            SPK_CUDA(cudaMemcpyAsync(d_first.p, &rows, sizeof(int), cudaMemcpyHostToDevice, s->stream));
-            k_aux_sweep<<<1, ((nc + 31) / 32) * 32, 0, s->stream>>>(p.ps, rl, p.pe, s->uia.p, s->uja.p, s->ua.p,
-                                                                    d_cols.p, nc, W.p);
-            k_aux_first<<<blocks_for(rows), 256, 0, s->stream>>>(rows, nc, W.p, tau, d_first.p);
-            SPK_CUDA(cudaGetLastError());
-            SPK_CUDA(cudaStreamSynchronize(s->stream));  // the stream does not sync with cudaMemcpy
-            int f = rows;
-            SPK_CUDA(cudaMemcpy(&f, d_first.p, sizeof(int), cudaMemcpyDeviceToHost));
-            aux_first[t] = f;
-        }
+    return SPK_OK;
+}
+
+bool aux_candidates(const spk_system *s) {
+    for (int t = 0; t < s->P; t++) {
+        const Part &p = s->parts[t];
+        const bool banded_trunc = (p.hasRefl || p.isOpt) && p.hasS && p.nRowsS > 0;
+        const int rl = p.maxIR;
+        if (!(banded_trunc || rl < p.ps || rl + 1 - p.ps < 256 || p.pe >= s->n)) return true;
     }
+    return false;
+}
+
+// The segment task lists of the partition solve from the first significant
+// spike rows and the internal spikes.
+int build_seg_tasks(spk_system *s, const std::vector<int> &first, const std::vector<int> &aux_first) {
+    const int P = s->P;
     std::vector<SegTask> t1, t2;
     long long rows1 = 0, rows2 = 0;
     for (int t = 0; t < P; t++) {
@@ -1855,6 +1843,61 @@ int solve_prepare(spk_system *s) {
     s->rows_phase4 = rows2;
     SPK_TRY(upload(s->d_tasks1, t1));
     SPK_TRY(upload(s->d_tasks2, t2));
+    return SPK_OK;
+}
+
+int solve_prepare(spk_system *s) {
+    const int P = s->P;
+    const double tau = s->trunc_tol;
+    auto wall_ms = []() {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch())
+            .count();
+    };
+    double lap = wall_ms();
+    auto mark = [&](int slot) {
+        const double t = wall_ms();
+        s->prep_ms[slot] = t - lap;
+        lap = t;
+    };
+    // first significant spike row per split block (rows above it: x = y)
+    std::vector<int> first(P, 0);
+    {
+        std::vector<int> plist, nr(P), nc(P);
+        std::vector<long long> ss(P);
+        for (int t = 0; t < P; t++) {
+            const Part &p = s->parts[t];
+            nr[t] = p.nRowsS;
+            nc[t] = p.nColsS;
+            ss[t] = p.startsS;
+            first[t] = p.nRowsS;
+            if (p.hasS && p.nRowsS > 0) plist.push_back(t);
+        }
+        if (tau >= 0 && !plist.empty()) {
+            DBuf<int> d_pl(s->stream), d_nr(s->stream), d_nc(s->stream), d_first(s->stream);
+            DBuf<long long> d_ss(s->stream);
+            SPK_TRY(upload(d_pl, plist));
+            SPK_TRY(upload(d_nr, nr));
+            SPK_TRY(upload(d_nc, nc));
+            SPK_TRY(upload(d_ss, ss));
+            SPK_TRY(upload(d_first, first));
+            dim3 grid(8, (unsigned)plist.size());
+            k_first_significant<<<grid, 256, 0, s->stream>>>((int)plist.size(), d_pl.p, d_ss.p, d_nr.p, d_nc.p,
+                                                              s->S.p, tau, d_first.p);
+            SPK_CUDA(cudaGetLastError());
+            SPK_CUDA(cudaStreamSynchronize(s->stream));
+            SPK_CUDA(cudaMemcpy(first.data(), d_first.p, sizeof(int) * P, cudaMemcpyDeviceToHost));
+        } else {
+            for (int t = 0; t < P; t++) first[t] = 0;
+        }
+    }
+    // internal spikes: computed here only when the partition solve is the
+    // default one (no chain plan, below); with chains they wait for the first
+    // partition-path use (partition_ensure), as only those solves read them
+    s->first_sig = first;
+    std::vector<int> aux_first(P, -1);
+    s->aux_pending = tau >= 0 && s->redNec && aux_candidates(s);
+    mark(1);  // first significant spike rows
+    SPK_TRY(build_seg_tasks(s, first, aux_first));
 
     // kept reduced rows, grouped by level in descending partition order
     std::vector<int> lvl(P + 1);
@@ -1884,6 +1927,7 @@ int solve_prepare(spk_system *s) {
 
     SPK_TRY(s->xbuf.alloc(s->n));
     if (s->uplo == 'L') SPK_TRY(s->xout_u.alloc(s->n));
+    mark(2);  // task lists, reduced levels, buffers
     // 1 / diagonal of U, padded to whole 32-row tiles (staged 256 bytes per tile)
     const int ntiles = (s->n + 31) / 32;
     SPK_TRY(s->rdiag.alloc(32ll * ntiles + 32));
@@ -1928,7 +1972,22 @@ int solve_prepare(spk_system *s) {
     SPK_CUDA(cudaStreamSynchronize(s->stream));
     SPK_TRY(s->d_err.alloc(1));
     SPK_CUDA(cudaMemset(s->d_err.p, 0, sizeof(int)));
-    return chain_prepare(s);
+    mark(3);  // 1/diagonal, sliced ELL
+    SPK_TRY(chain_prepare(s));
+    if (!s->chain_ok) SPK_TRY(partition_ensure(s));
+    mark(4);  // chain layout, spikes and plans (or the internal spikes without chains)
+    return SPK_OK;
+}
+
+// Internal spikes and the task lists that use them, before the first solve on
+// the partition path (a no-op once done, or when no block needs them).
+int partition_ensure(spk_system *s) {
+    if (!s->aux_pending) return SPK_OK;
+    std::vector<int> aux_first;
+    SPK_TRY(aux_spikes(s, aux_first));
+    SPK_TRY(build_seg_tasks(s, s->first_sig, aux_first));
+    s->aux_pending = 0;
+    return SPK_OK;
 }
 
 namespace {
@@ -2168,6 +2227,7 @@ int solve(spk_system *s, const double *b, double *x, cudaStream_t st, double *ph
         set_error(SPK_ERR_STATE, "no preprocessed system");
         return SPK_ERR_STATE;
     }
+    if (!(s->chain_ok && (!ph || s->lean))) SPK_TRY(partition_ensure(s));  // the partition path below
     double t0 = 0;
     auto lap = [&](int slot) {
         if (!ph) return;
@@ -2339,6 +2399,7 @@ int solve_batch(spk_system *s, int nrhs, const double *B, long long ldb, double 
     const bool use_chain =
         s->chain_ok && (s->lean || (s->batch_path >= 0 ? s->batch_path == 1
                                                        : (cb ? cb[0] == '1' : (mode == 0 || !part_wide))));
+    if (!use_chain) SPK_TRY(partition_ensure(s));
     if (use_chain) {
         // the chain tasks fill the GPU whatever the partition count: every group
         // of up to 32 columns is one right-hand-side-parallel chain solve (used
@@ -2852,6 +2913,7 @@ int spk_group_create(spk_group **out, int count, spk_system *const *systems, con
             set_error(SPK_ERR_STATE, "group member %d was compacted (spk_compact): groups need the partition pools", i);
             return fail(SPK_ERR_STATE);
         }
+        if (const int rc = partition_ensure(s); rc != SPK_OK) return fail(rc);
         if (mode == 1) {
             int rc = ensure_fp32(s);
             if (rc == SPK_OK) rc = ensure_residual(s);

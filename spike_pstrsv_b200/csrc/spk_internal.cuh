@@ -192,6 +192,14 @@ struct spk_system {
     spk::ChainPlan cp_batch;  // the batched kernel's own chains (longer; built at preprocessing)
     spk::ChainPlan cp_host;   // the host-array pipeline's chains (shorter; built on first use)
     int batch_path = -1;      // spk_tune "batch_path": 1 chain kernels, 0 partition kernels, -1 automatic
+    // wall milliseconds of the last preprocessing: the reference's steps, first
+    // significant spike rows + internal spikes, reduced levels + buffers, the
+    // sliced-ELL layout, the chain layout and plans (spk_debug_scalar "prep_us_*")
+    double prep_ms[5] = {0, 0, 0, 0, 0};
+    // first significant spike row per block; internal spikes not yet computed
+    // (the partition solve's task lists are then untruncated on those blocks)
+    std::vector<int> first_sig;
+    int aux_pending = 0;
     int host_plan_tried = 0;
     int nctasks1 = 0, nctasks4 = 0;
     long long ch_rows1 = 0, ch_rows4 = 0;
@@ -236,6 +244,7 @@ int solve_prepare(spk_system *s);
 int residual_prepare(spk_system *s);
 int chain_prepare(spk_system *s);
 int chain_tune(spk_system *s, const char *name, long long v);
+int partition_ensure(spk_system *s);
 int chain_solve(spk_system *s, const double *b, double *x, cudaStream_t st, bool prof, int ring);
 int chain_solve_host(spk_system *s, const double *b, double *x, double *db, double *dx);
 long long chain_device_check();
