@@ -20,3 +20,22 @@ def test_driver_links_and_prints_usage(path):
     out = subprocess.run([path], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0, out.stderr
     assert out.stdout.startswith("Usage:")
+
+
+def test_every_compat_symbol_is_exported():
+    """Every function include/compat/mkl.h declares is exported by
+    libspike_pstrsv_mklcompat.so (the MKL entry points the reference's drivers call)."""
+    import re
+
+    from conftest import ROOT
+    from spike_pstrsv_b200 import build
+
+    text = open(os.path.join(ROOT, "include", "compat", "mkl.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    funcs = set(re.findall(r"^\s*(?:const\s+)?[a-z_]+\s*\**\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, flags=re.M))
+    assert {"mkl_cspblas_dcsrtrsv", "mkl_sparse_d_trsv", "mkl_sparse_d_create_csr", "mkl_dcsrmv",
+            "cblas_dcopy", "mkl_malloc", "mkl_free"} <= funcs
+    lib = build.build_compat()
+    out = subprocess.run(["nm", "-D", "--defined-only", lib], capture_output=True, text=True, check=True)
+    exported = {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+    assert sorted(funcs - exported) == []
