@@ -344,12 +344,18 @@ void worker(spk_server *S, Slot *sl) {
             if (status == SPK_OK && !(resid >= 0 && resid <= kTol)) {
                 // not at the tolerance (FP32 refinement that stalls, or a bad
                 // batch): solve it again in FP64 and check; fail it if still above
+                const double first_resid = resid;
                 lk.unlock();
                 status = run_batch(S, sl, M, batch, SPK_MODE_FP64, &iters, &resid);
                 lk.lock();
                 S->rechecks++;
                 if (status == SPK_OK && !(resid >= 0 && resid <= kTol)) {
                     set_error(SPK_ERR_INPUT, "batch scaled residual %.3e above %.0e", resid, kTol);
+                    // the requests fail; the log keeps what the caller's status cannot
+                    fprintf(stderr,
+                            "spk server: matrix %d (n=%d, %zu requests): scaled residual %.3e after mode %d, "
+                            "%.3e after FP64; the requests fail\n",
+                            M->id, M->n, batch.size(), first_resid, mode, resid);
                     status = SPK_ERR_INPUT;
                 }
             }
