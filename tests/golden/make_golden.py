@@ -8,7 +8,8 @@ reference's globals that the structure tests compare).
 
 * ``small_*.npz``  full arrays (small matrices).
 * ``digest.json``  SHA-256 of every structure array plus the scalar fields, for
-  the BASELINE-sized cases (Poisson 128x128 at 4 partitions, banded 65,536 rows).
+  the benchmark-sized cases (Poisson 128x128 at 4 partitions, banded 65,536 rows,
+  and the full banded workload of 4,194,304 rows).
 
 'L' cases run the reference's 'U' path on the reversal mirror J L J (the
 reference's own 'L' path is unimplemented, src/spike_pstrsv.c:234-237).
